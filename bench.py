@@ -1,0 +1,392 @@
+"""Benchmark of the SMD path: SMD site-steps/s on the triangular-lattice
+workload (c2: L=48, N=2304, 64 samples per GPU, FP32 precision form, FP64
+correction every 16 steps, 48 x 48 grid + 512-point path, 4096 records).
+
+One bench step = one full job over the batch: RK4 integration of every
+sample, the per-record projection onto all q, the windowed time transform
+and the sample accumulation of |S(q,w)|^2.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload c2] [--no-cpu-baseline]
+
+Under torchrun every rank integrates its own 64 samples (weak scaling); the
+sample sums are added across ranks with one NCCL all-reduce per step, the
+multi-GPU form of the reference's end-of-run MPI reduction
+(Codes_Folder/smd_code.cpp:3332-3397).  Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SMD site-steps/s"
+UNIT = "site-steps/s"
+
+
+def flops_per_site_step(z: int) -> int:
+    """Algorithmic flops of one site-step of RK4 + energy correction: 6 field
+    sweeps x 6z, 4 stages x 18, combine and normalise 24, correction 53,
+    energy sums 6z (Codes_Folder/subrouts.cpp:11734-11902)."""
+    return 42 * z + 150
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if p[5 + k].lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# --------------------------------------------------------- CPU reference
+
+def reference_runner_step(w, procs: int, ntm: int, workdir: str):
+    """The reference's own SMD code (oracle/_ref/smd_ref_run, built from
+    Codes_Folder/subrouts.cpp) on `procs` host cores: one single-rank process
+    per core, each integrating one sample of the workload's lattice for
+    ntm - 1 steps (every step recorded, as the reference does), like the
+    reference's MPI sample decomposition (Codes_Folder/smd_code.cpp:3130-3180).
+    Returns (site_steps, max_ms)."""
+    runner = os.path.join(ROOT, "oracle", "_ref", "smd_ref_run")
+    jobs = []
+    for p in range(procs):
+        args = [runner, workdir, os.path.join(workdir, "samples.bin"), str(p), "1",
+                "--no-dwf-guard"]
+        jobs.append(subprocess.Popen(args, stdout=subprocess.PIPE, stderr=subprocess.PIPE,
+                                     text=True))
+    ms = []
+    for j in jobs:
+        out, err = j.communicate()
+        if j.returncode != 0:
+            raise RuntimeError(f"reference runner failed: {err.strip()[-300:]}")
+        ms.append(json.loads(out.strip().splitlines()[-1])["rk_loop_ms"])
+    N = w.settings.N
+    return procs * N * (ntm - 1), max(ms)
+
+
+def prepare_reference(w, procs: int, ntm: int):
+    from classical_mc_and_smd_for_2d_heisenberg_models_b200 import samples as smp
+    import dataclasses
+    s = dataclasses.replace(w.settings, ntm=ntm, window=w.window,
+                            NMeas=1000 * max(2, procs), crSkip=1000, imp_ratio=0.0)
+    wd = tempfile.mkdtemp(prefix="smd_ref_")
+    s.write(wd)
+    spins, _ = smp.make_samples(s, procs, w.state, w.sigma, w.seed)
+    smp.write_sample_file(os.path.join(wd, "samples.bin"), s, spins, None)
+    return wd
+
+
+def reference_available() -> bool:
+    return os.access(os.path.join(ROOT, "oracle", "_ref", "smd_ref_run"), os.X_OK)
+
+
+def ref_procs() -> int:
+    return max(1, min(os.cpu_count() or 1, 64))
+
+
+# ------------------------------------------------------------------ ours
+
+def run_ours(args, w, rank, world):
+    import torch
+    from classical_mc_and_smd_for_2d_heisenberg_models_b200 import _lib, smd, workloads
+    import ctypes as C
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    s = w.settings
+    lat = smd.build_lattice(s.geom, s.L)
+    spins, imp = workloads.make_inputs(w, rank)
+    win = smd.window(w.window, w.n_rec)
+    ql = workloads.path_points(s.geom, w.qpath_points) if w.qpath_points else None
+    ctx = smd.Context(local)
+    lid = ctx.lattice(s, lat)
+    qid = ctx.qset(lid, use_grid=True, qlist=ql)
+    Q = ctx.qset_size(qid)
+    S, N, n = w.n_samples, s.N, w.n_rec
+    lib = ctx.lib
+
+    # device-resident inputs and accumulators
+    d_spins = torch.from_numpy(spins).to(f"cuda:{local}")
+    d_win = torch.from_numpy(win).to(f"cuda:{local}")
+    d_spec = torch.zeros((3, Q, n), dtype=torch.float64, device=f"cuda:{local}")
+    d_qss = torch.zeros(n, dtype=torch.float64, device=f"cuda:{local}")
+    imp_arr = None if imp is None else np.ascontiguousarray(imp, np.int32)
+
+    def device_step(precision, fix_every):
+        d_spec.zero_()
+        d_qss.zero_()
+        torch.cuda.synchronize()
+        j = ctx.job(lid, qid, S, s.dtm, n, w.stride, precision, fix_every, imp_arr)
+        rep = _lib.Report()
+        rc = lib.smd_run_device(ctx.h, C.byref(j), C.c_void_p(d_spins.data_ptr()),
+                                C.c_void_p(d_win.data_ptr()), C.c_void_p(d_spec.data_ptr()),
+                                C.c_void_p(d_qss.data_ptr()), None, C.byref(rep))
+        if rc:
+            raise _lib.SMDError(rc, lib.smd_last_error(ctx.h).decode())
+        if dist is not None:
+            dist.all_reduce(d_spec)
+            dist.all_reduce(d_qss)
+        torch.cuda.synchronize()
+        return rep
+
+    # ---- precision form, device-resident (value)
+    for _ in range(args.warmup):
+        device_step(w.precision, w.fix_every)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    reps = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            reps.append(device_step(w.precision, w.fix_every))
+        torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    ms_dev = sum(r.ms_device for r in reps)
+    ms_rk = sum(r.ms_rk for r in reps)
+    rk_launches = sum(r.rk_launches for r in reps)
+    launches = sum(r.kernel_launches for r in reps)
+    drift_max = max(r.drift_max for r in reps)
+    drift_final = max(r.drift_final for r in reps)
+    t = torch.tensor([ms_dev], dtype=torch.float64, device=f"cuda:{local}")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    site_steps_rank = float(S) * N * w.steps
+    total_site_steps = site_steps_rank * world * args.steps
+    value = total_site_steps / (ms_max / 1e3)
+    samples_per_s = (S * world * args.steps) / (ms_max / 1e3)
+
+    # ---- e2e through the C ABI with pinned host buffers (smd_run)
+    pin_in = torch.from_numpy(spins).pin_memory()
+    pin_win = torch.from_numpy(win).pin_memory()
+    pin_spec = torch.zeros((3, Q, n), dtype=torch.float64).pin_memory()
+    pin_qss = torch.zeros(n, dtype=torch.float64).pin_memory()
+    dp = lambda tns: C.cast(C.c_void_p(tns.data_ptr()), C.POINTER(C.c_double))
+
+    def e2e_step():
+        j = ctx.job(lid, qid, S, s.dtm, n, w.stride, w.precision, w.fix_every, imp_arr)
+        rep = _lib.Report()
+        t0 = time.perf_counter()
+        rc = lib.smd_run(ctx.h, C.byref(j), dp(pin_in), dp(pin_win), dp(pin_spec), dp(pin_qss),
+                         None, C.byref(rep))
+        t1 = time.perf_counter()
+        if rc:
+            raise _lib.SMDError(rc, lib.smd_last_error(ctx.h).decode())
+        return t1 - t0
+
+    e2e_steps = max(1, min(args.steps, 3))
+    e2e_step()
+    e2e_t = [e2e_step() for _ in range(e2e_steps)]
+    tt = torch.tensor([max(e2e_t)], dtype=torch.float64, device=f"cuda:{local}")
+    if dist is not None:
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    e2e_value = site_steps_rank * world / float(tt.item())
+    h2d = spins.nbytes + win.nbytes
+    d2h = 3 * Q * n * 8 + n * 8
+
+    # ---- FP64 plain form on the same workload (the 4x target's denominator)
+    fp64 = None
+    if not args.no_fp64:
+        device_step(_lib.SMD_FP64, 1)
+        r64 = [device_step(_lib.SMD_FP64, 1) for _ in range(max(1, min(args.steps, 2)))]
+        ms64 = sum(r.ms_device for r in r64)
+        t64 = torch.tensor([ms64], dtype=torch.float64, device=f"cuda:{local}")
+        if dist is not None:
+            dist.all_reduce(t64, op=dist.ReduceOp.MAX)
+        fp64_value = site_steps_rank * world * len(r64) / (float(t64.item()) / 1e3)
+        fp64 = {"value": fp64_value, "unit": UNIT,
+                "ms_per_step": float(t64.item()) / len(r64),
+                "ms_rk_per_step": sum(r.ms_rk for r in r64) / len(r64),
+                "ms_proj_per_step": sum(r.ms_proj for r in r64) / len(r64),
+                "ms_tfft_per_step": sum(r.ms_tfft for r in r64) / len(r64),
+                "drift_max_per_site": max(r.drift_max for r in r64)}
+
+    # ---- roofline of the dominant kernel (RK4 + correction)
+    z = sum(lat.zn[k] for k, on in enumerate([True, s.j2_on, s.jx_on]) if on)
+    fpss = flops_per_site_step(z)
+    peak = C.c_double()
+    prec_peak = lib.smd_measure_fma_peak(local, w.precision, C.byref(peak))
+    rk_flops = fpss * site_steps_rank * args.steps
+    achieved = rk_flops / (ms_rk / 1e3) / 1e12
+    roof = {"kernel": "rk_fp32_kernel" if w.precision == _lib.SMD_FP32 else "rk_fp64_kernel",
+            "bound": "fp32" if w.precision == _lib.SMD_FP32 else "fp64",
+            "achieved": achieved, "peak": peak.value if prec_peak == 0 else None,
+            "unit": "TFLOP/s",
+            "frac": (achieved / peak.value) if prec_peak == 0 and peak.value > 0 else None,
+            "peak_source": "smd_measure_fma_peak (FMA chains on every SM)",
+            "algorithmic_flops_per_site_step": fpss,
+            "avg_launch_ms": ms_rk / max(1, rk_launches),
+            "traffic": None}
+
+    if dist is not None:
+        dist.destroy_process_group()
+    ctx.close()
+
+    line = None
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 stages / f64 master+energy",
+            "data": "synthetic (seeded 120-degree states with 0.15 rad Gaussian tilts)",
+            "config": {"workload": w.describe(), "samples_per_gpu": S,
+                       "rk_steps": w.steps, "records": n, "Q": Q,
+                       "l2": "inputs larger than L2 (time series %.1f GB per GPU)" %
+                             (S * 3 * n * Q * 8 / 1e9),
+                       "parallelism": f"samples sharded over {world} GPU(s)"},
+            "dssf_samples_per_s": samples_per_s,
+            "breakdown_ms_per_step": {"device": ms_dev / args.steps, "rk": ms_rk / args.steps,
+                                      "proj": sum(r.ms_proj for r in reps) / args.steps,
+                                      "tfft": sum(r.ms_tfft for r in reps) / args.steps},
+            "energy_drift_per_site": {"max": drift_max, "final": drift_final},
+            "fp64_plain": fp64,
+            "speedup_vs_fp64_plain": (value / fp64["value"]) if fp64 else None,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": float(tt.item()) * 1e3},
+            "roofline": roof,
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+    return line
+
+
+def cpu_baseline(w, args):
+    """Bounded sample of the reference's own CPU code, all host cores."""
+    if not reference_available():
+        return {"value": None, "unavailable": "oracle/_ref/smd_ref_run not built"}
+    procs = ref_procs()
+    ntm = args.ref_ntm
+    wd = prepare_reference(w, procs, ntm)
+    site_steps, ms = reference_runner_step(w, procs, ntm, wd)
+    return {"value": site_steps / (ms / 1e3), "unit": UNIT, "cores": procs, "kind": "reference",
+            "sample": f"{procs} processes x 1 sample x {ntm - 1} RK steps of {w.name} "
+                      f"(N={w.settings.N}), every step recorded; reference code, "
+                      f"non-MKL DFT (MKL not available on this box)"}
+
+
+def run_reference_arm(args, w, rank, world):
+    if rank != 0:
+        return None
+    if not reference_available():
+        return {"impl": "reference", "unavailable": "reference runner not built on this box"}
+    procs = ref_procs()
+    ntm = args.ref_ntm
+    wd = prepare_reference(w, procs, ntm)
+    for _ in range(args.warmup):
+        reference_runner_step(w, procs, ntm, wd)
+    tot, tmax = 0.0, 0.0
+    for _ in range(args.steps):
+        ss, ms = reference_runner_step(w, procs, ntm, wd)
+        tot += ss
+        tmax += ms
+    value = tot / (tmax / 1e3)
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": tmax / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded 120-degree states with 0.15 rad Gaussian tilts)",
+        "config": {"workload": w.describe(), "samples_per_step": procs, "rk_steps": ntm - 1},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "reference",
+                         "sample": f"{procs} processes x 1 sample x {ntm - 1} RK steps per step"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2")
+    ap.add_argument("--ref-ntm", type=int, default=1025)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    from classical_mc_and_smd_for_2d_heisenberg_models_b200 import workloads
+    w = workloads.WORKLOADS[args.workload]()
+    if args.impl == "reference":
+        line = run_reference_arm(args, w, rank, world)
+    else:
+        line = run_ours(args, w, rank, world)
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(w, args)
+    if rank == 0 and line is not None:
+        print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,814 @@
+// host.cu -- C ABI of the SMD library: context, lattice and q-set upload,
+// and the job pipeline.
+//
+// A job (the reference's RK loop over samples, Codes_Folder/smd_code.cpp:
+// 3079-3291, with get_dynSpectrum per sample) runs in waves of W samples that
+// fit the context's HBM budget.  Within a wave the records are produced in
+// chunks of R records:
+//
+//   stream rk   : RK kernel, one CTA per sample, writes the chunk's spin
+//                 snapshots into one of two snapshot buffers
+//   stream proj : grid projection (2D FFT) and list projection of the chunk,
+//                 writing S(q,t) into the wave's time series
+//
+// so the projection of chunk c overlaps the integration of chunk c+1 on the
+// SMs the RK kernel leaves free.  After the last chunk the time-FFT kernel
+// windows, transforms and squares every series and adds the sum over the
+// wave's samples into the job's accumulator.
+#include "../../include/smd_b200.h"
+#include "smd_launch.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <set>
+#include <string>
+#include <tuple>
+#include <vector>
+
+using namespace smd;
+
+namespace {
+
+const char *kVersion = "smd_b200 0.1 (sm_100a)";
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    ~DevBuf() { release(); }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    cudaError_t ensure(size_t b)
+    {
+        if (b <= bytes) return cudaSuccess;
+        release();
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e == cudaSuccess) bytes = b;
+        else p = nullptr;
+        return e;
+    }
+    template <typename T>
+    T *as() const { return static_cast<T *>(p); }
+};
+
+struct Lattice {
+    int N = 0, G = 0, zn[3] = {0, 0, 0}, zoff[3] = {0, 0, 0}, ztot = 0;
+    bool lieb_delta = false;
+    LatticeDev dev{};
+    DevBuf nbr, grid_map, bonds;
+    std::vector<double> pos;
+};
+
+struct QSet {
+    int lattice = -1;
+    int use_grid = 0;
+    int G = 0;
+    int n_list = 0;
+    int Q = 0;
+    double list_scale = 1.0;
+    int fp64_ok = 1;           // the FP64 grid transform fits one CTA
+    FFTPlan gplan{};
+    DevBuf tw64, tw32;        // grid twiddles
+    DevBuf phase64, phase32;  // [N][n_list] complex
+};
+
+struct Plan {
+    FFTPlan p{};
+    DevBuf tw64, tw32;
+};
+
+}  // namespace
+
+struct smd_ctx {
+    int device = 0;
+    size_t budget = 0;
+    cudaStream_t s_rk = nullptr, s_proj = nullptr;
+    cudaEvent_t ev_rk[2] = {nullptr, nullptr}, ev_proj[2] = {nullptr, nullptr};
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    std::string err;
+    int next_id = 1;
+    std::map<int, std::unique_ptr<Lattice>> lattices;
+    std::map<int, std::unique_ptr<QSet>> qsets;
+    std::map<int, std::unique_ptr<Plan>> tplans;   // keyed by n
+    // job buffers (grow-only)
+    DevBuf state, s0, imp, snap[2], series, qss, stats, e0, status, win, acc_tmp, in_tmp, out_tmp;
+    int launches = 0;
+    std::vector<cudaEvent_t> tev;   // timing events, reused across calls
+};
+
+namespace {
+
+int fail(smd_ctx *c, int code, const std::string &msg)
+{
+    if (c) c->err = msg;
+    return code;
+}
+
+int cuda_fail(smd_ctx *c, cudaError_t e, const char *where)
+{
+    return fail(c, SMD_ECUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(expr, where)                                   \
+    do {                                                  \
+        cudaError_t _e = (expr);                          \
+        if (_e != cudaSuccess) return cuda_fail(ctx, _e, where); \
+    } while (0)
+
+bool make_plan(int n, FFTPlan &p)
+{
+    p.n = n;
+    p.nst = 0;
+    int m = n;
+    while (m % 4 == 0 && m > 4 && p.nst < 16) { p.radix[p.nst++] = 4; m /= 4; }
+    for (int r : {4, 2, 3, 5}) {
+        while (m % r == 0 && m > 1 && p.nst < 16) { p.radix[p.nst++] = r; m /= r; }
+    }
+    for (int r = 7; m > 1 && p.nst < 16; r += 2) {
+        while (m % r == 0 && p.nst < 16) {
+            if (r > 64) return false;   // large primes are not supported
+            p.radix[p.nst++] = r;
+            m /= r;
+        }
+    }
+    return m == 1;
+}
+
+// exp(-2 pi i j / n) for j < n, accurate to one rounding
+void twiddles(int n, std::vector<double> &w)
+{
+    w.resize(2 * (size_t)n);
+    const double two_pi = 2.0 * std::acos(-1.0);
+    for (int j = 0; j < n; j++) {
+        const long jj = (2L * j > n) ? (long)j - n : j;
+        const double a = two_pi * (double)jj / (double)n;
+        w[2 * j] = std::cos(a);
+        w[2 * j + 1] = -std::sin(a);
+    }
+}
+
+cudaError_t upload_twiddles(int n, DevBuf &d64, DevBuf &d32)
+{
+    std::vector<double> w;
+    twiddles(n, w);
+    std::vector<float> wf(w.begin(), w.end());
+    cudaError_t e = d64.ensure(w.size() * sizeof(double));
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpy(d64.p, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return e;
+    e = d32.ensure(wf.size() * sizeof(float));
+    if (e != cudaSuccess) return e;
+    return cudaMemcpy(d32.p, wf.data(), wf.size() * sizeof(float), cudaMemcpyHostToDevice);
+}
+
+// E = 1/2 sum_i (S_i . h_i - h S_i^z) equals the bond sum when every
+// neighbour relation is a bond listed once, present in both directions in
+// the same shell, with one coupling sign.
+bool field_energy_identity(const smd_lattice_desc *d)
+{
+    const int N = d->N;
+    std::map<std::tuple<int, int>, std::pair<int, int>> edges;   // (i,j) -> (shell, count)
+    std::map<std::tuple<int, int>, int> sign;                    // Lieb d-wave sign per edge
+    for (int s = 0; s < 3; s++) {
+        if (!d->shell_on[s]) continue;
+        for (int i = 0; i < N; i++)
+            for (int k = 0; k < d->zn[s]; k++) {
+                const int j = d->nbr[s][i * d->zn[s] + k];
+                if (j < 0 || j == i) return false;
+                auto key = std::make_tuple(i, j);
+                auto it = edges.find(key);
+                if (it != edges.end()) return false;   // duplicate neighbour
+                edges[key] = {s, 1};
+                sign[key] = ((i & 1) ? -1 : 1) * ((k & 1) ? -1 : 1);
+            }
+    }
+    for (auto &e : edges) {
+        const int i = std::get<0>(e.first), j = std::get<1>(e.first);
+        auto r = edges.find(std::make_tuple(j, i));
+        if (r == edges.end() || r->second.first != e.second.first) return false;
+        if (d->lieb_delta_on && e.second.first == 1) {
+            const int bond_sign = ((i & 1) ? -1 : 1) * ((j & 1) ? -1 : 1);
+            if (sign[e.first] != bond_sign || sign[r->first] != bond_sign) return false;
+        }
+    }
+    // the bond list holds every undirected edge once, in its shell
+    const int nb = d->nbonds[0] + d->nbonds[1] + d->nbonds[2];
+    if ((size_t)nb * 2 != edges.size()) return false;
+    int b = 0;
+    for (int s = 0; s < 3; s++)
+        for (int q = 0; q < d->nbonds[s]; q++, b++) {
+            const int i = d->bonds[2 * b], j = d->bonds[2 * b + 1];
+            auto it = edges.find(std::make_tuple(i, j));
+            if (it == edges.end() || it->second.first != s) return false;
+        }
+    return true;
+}
+
+}  // namespace
+
+// ====================================================================== ABI
+
+extern "C" const char *smd_version(void) { return kVersion; }
+
+extern "C" const char *smd_last_error(const smd_ctx *ctx)
+{
+    return ctx ? ctx->err.c_str() : "null context";
+}
+
+extern "C" int smd_ctx_create(const smd_device_opts *opts, smd_ctx **out)
+{
+    if (!out) return SMD_EINVAL;
+    *out = nullptr;
+    std::unique_ptr<smd_ctx> c(new smd_ctx());
+    smd_ctx *ctx = c.get();
+    c->device = opts ? opts->device : 0;
+    int ndev = 0;
+    CK(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
+    if (c->device < 0 || c->device >= ndev) return SMD_EINVAL;
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, c->device), "cudaGetDeviceProperties");
+    if (prop.major != 10) {
+        // the kernels are built for sm_100a only
+        return SMD_EINVAL;
+    }
+    size_t fr = 0, tot = 0;
+    CK(cudaMemGetInfo(&fr, &tot), "cudaMemGetInfo");
+    c->budget = (opts && opts->hbm_budget) ? opts->hbm_budget : (size_t)(0.85 * (double)fr);
+    CK(cudaStreamCreateWithFlags(&c->s_rk, cudaStreamNonBlocking), "stream");
+    CK(cudaStreamCreateWithFlags(&c->s_proj, cudaStreamNonBlocking), "stream");
+    for (int i = 0; i < 2; i++) {
+        CK(cudaEventCreateWithFlags(&c->ev_rk[i], cudaEventDisableTiming), "event");
+        CK(cudaEventCreateWithFlags(&c->ev_proj[i], cudaEventDisableTiming), "event");
+    }
+    CK(cudaEventCreate(&c->t0), "event");
+    CK(cudaEventCreate(&c->t1), "event");
+    *out = c.release();
+    return SMD_OK;
+}
+
+extern "C" int smd_ctx_destroy(smd_ctx *ctx)
+{
+    if (!ctx) return SMD_EINVAL;
+    cudaSetDevice(ctx->device);
+    cudaDeviceSynchronize();
+    ctx->lattices.clear();
+    ctx->qsets.clear();
+    ctx->tplans.clear();
+    for (int i = 0; i < 2; i++) {
+        cudaEventDestroy(ctx->ev_rk[i]);
+        cudaEventDestroy(ctx->ev_proj[i]);
+    }
+    for (cudaEvent_t e : ctx->tev) cudaEventDestroy(e);
+    cudaEventDestroy(ctx->t0);
+    cudaEventDestroy(ctx->t1);
+    cudaStreamDestroy(ctx->s_rk);
+    cudaStreamDestroy(ctx->s_proj);
+    delete ctx;
+    return SMD_OK;
+}
+
+extern "C" int smd_lattice_upload(smd_ctx *ctx, const smd_lattice_desc *d, int *lattice_id)
+{
+    if (!ctx || !d || !lattice_id) return SMD_EINVAL;
+    if (d->N <= 0) return fail(ctx, SMD_EINVAL, "lattice: N must be positive");
+    for (int s = 0; s < 3; s++) {
+        if (d->zn[s] < 0 || d->zn[s] > 6) return fail(ctx, SMD_EINVAL, "lattice: zn must lie in [0, 6]");
+        if (d->shell_on[s] && d->zn[s] > 0 && !d->nbr[s])
+            return fail(ctx, SMD_EINVAL, "lattice: missing neighbour table");
+    }
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    auto L = std::make_unique<Lattice>();
+    const int N = d->N;
+    L->N = N;
+    L->G = d->G;
+    int z = 0;
+    for (int s = 0; s < 3; s++) {
+        L->zn[s] = d->shell_on[s] ? d->zn[s] : 0;
+        L->zoff[s] = z;
+        z += L->zn[s];
+    }
+    L->ztot = z;
+    // ELL [ztot][N]
+    std::vector<int> ell((size_t)std::max(z, 1) * N, -1);
+    for (int s = 0; s < 3; s++)
+        for (int k = 0; k < L->zn[s]; k++)
+            for (int i = 0; i < N; i++) {
+                const int j = d->nbr[s][i * d->zn[s] + k];
+                if (j >= N) return fail(ctx, SMD_EINVAL, "lattice: neighbour index out of range");
+                ell[(size_t)(L->zoff[s] + k) * N + i] = j;
+            }
+    CK(L->nbr.ensure(ell.size() * sizeof(int)), "cudaMalloc");
+    CK(cudaMemcpy(L->nbr.p, ell.data(), ell.size() * sizeof(int), cudaMemcpyHostToDevice), "H2D");
+    if (d->G > 0) {
+        if (!d->grid_map) return fail(ctx, SMD_EINVAL, "lattice: G > 0 needs grid_map");
+        for (int k = 0; k < d->G * d->G; k++)
+            if (d->grid_map[k] >= N) return fail(ctx, SMD_EINVAL, "lattice: grid map out of range");
+        CK(L->grid_map.ensure((size_t)d->G * d->G * sizeof(int)), "cudaMalloc");
+        CK(cudaMemcpy(L->grid_map.p, d->grid_map, (size_t)d->G * d->G * sizeof(int),
+                      cudaMemcpyHostToDevice), "H2D");
+    }
+    const int nb = d->nbonds[0] + d->nbonds[1] + d->nbonds[2];
+    std::vector<int4> bonds((size_t)std::max(nb, 1));
+    {
+        int b = 0;
+        for (int s = 0; s < 3; s++)
+            for (int q = 0; q < d->nbonds[s]; q++, b++) {
+                const int i = d->bonds[2 * b], j = d->bonds[2 * b + 1];
+                if (i < 0 || j < 0 || i >= N || j >= N)
+                    return fail(ctx, SMD_EINVAL, "lattice: bond index out of range");
+                bonds[b] = make_int4(i, j, s, 0);
+            }
+    }
+    CK(L->bonds.ensure(bonds.size() * sizeof(int4)), "cudaMalloc");
+    CK(cudaMemcpy(L->bonds.p, bonds.data(), bonds.size() * sizeof(int4), cudaMemcpyHostToDevice), "H2D");
+    if (d->pos) L->pos.assign(d->pos, d->pos + 2 * (size_t)N);
+
+    LatticeDev &v = L->dev;
+    std::memset(&v, 0, sizeof v);
+    v.N = N;
+    for (int s = 0; s < 3; s++) {
+        v.zn[s] = L->zn[s];
+        v.zoff[s] = L->zoff[s];
+        v.shell_on[s] = d->shell_on[s] && L->zn[s] > 0;
+        for (int a = 0; a < 2; a++)
+            for (int b = 0; b < 2; b++) {
+                v.J[s][a][b] = d->J[s][a][b];
+                v.Jf[s][a][b] = (float)d->J[s][a][b];
+            }
+        for (int c = 0; c < 3; c++) {
+            v.lam[s][c] = d->lambda[s][c];
+            v.lamf[s][c] = (float)d->lambda[s][c];
+            v.coef[s][c] = d->J[s][0][0] * d->lambda[s][c];
+            v.coeff[s][c] = (float)v.coef[s][c];
+        }
+    }
+    v.ztot = z;
+    v.nbr = L->nbr.as<int>();
+    v.lieb_delta_on = d->lieb_delta_on && std::fabs(d->j2_delta) > 1.0e-12;
+    v.j2_delta = d->j2_delta;
+    v.j2_deltaf = (float)d->j2_delta;
+    v.h = std::fabs(d->h) > 1.0e-12 ? d->h : 0.0;   // extH_ON, subrouts.cpp:1282-1285
+    v.hf = (float)v.h;
+    v.energy_from_field = field_energy_identity(d) ? 1 : 0;
+    v.nbonds = nb;
+    v.bonds = L->bonds.as<int4>();
+    L->lieb_delta = v.lieb_delta_on;
+    const int id = ctx->next_id++;
+    ctx->lattices[id] = std::move(L);
+    *lattice_id = id;
+    return SMD_OK;
+}
+
+extern "C" int smd_lattice_free(smd_ctx *ctx, int lattice_id)
+{
+    if (!ctx) return SMD_EINVAL;
+    cudaSetDevice(ctx->device);
+    cudaDeviceSynchronize();
+    if (!ctx->lattices.erase(lattice_id)) return SMD_ENOTFOUND;
+    return SMD_OK;
+}
+
+extern "C" int smd_qset_upload(smd_ctx *ctx, int lattice_id, int use_grid, int n_list,
+                               const double *qlist, double list_scale, int *qset_id)
+{
+    if (!ctx || !qset_id) return SMD_EINVAL;
+    auto it = ctx->lattices.find(lattice_id);
+    if (it == ctx->lattices.end()) return fail(ctx, SMD_ENOTFOUND, "qset: unknown lattice");
+    Lattice &L = *it->second;
+    if (n_list < 0 || (n_list > 0 && !qlist)) return fail(ctx, SMD_EINVAL, "qset: bad q list");
+    if (n_list > 0 && L.pos.empty()) return fail(ctx, SMD_EINVAL, "qset: lattice has no positions");
+    if (use_grid && L.G <= 0) return fail(ctx, SMD_EINVAL, "qset: lattice has no DFT grid");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    auto Q = std::make_unique<QSet>();
+    Q->lattice = lattice_id;
+    Q->use_grid = use_grid ? 1 : 0;
+    Q->G = use_grid ? L.G : 0;
+    Q->n_list = n_list;
+    Q->Q = Q->G * Q->G + n_list;
+    Q->list_scale = list_scale;
+    if (Q->Q <= 0) return fail(ctx, SMD_EINVAL, "qset: empty");
+    if (use_grid) {
+        if (!make_plan(L.G, Q->gplan)) return fail(ctx, SMD_EINVAL, "qset: grid size has a prime factor > 64");
+        if ((size_t)L.G * L.G > 16384) return fail(ctx, SMD_EINVAL, "qset: grid larger than 128 x 128");
+        if ((size_t)L.G * L.G > 8192 || grid_proj_smem(L.G, 0, Q->gplan) > 200 * 1024)
+            Q->fp64_ok = 0;
+        CK(upload_twiddles(L.G, Q->tw64, Q->tw32), "twiddles");
+    }
+    if (n_list > 0) {
+        const int N = L.N;
+        std::vector<double> ph((size_t)N * n_list * 2);
+        for (int k = 0; k < N; k++)
+            for (int l = 0; l < n_list; l++) {
+                const double a = -(qlist[2 * l] * L.pos[2 * k] + qlist[2 * l + 1] * L.pos[2 * k + 1]);
+                ph[2 * ((size_t)k * n_list + l)] = list_scale * std::cos(a);
+                ph[2 * ((size_t)k * n_list + l) + 1] = list_scale * std::sin(a);
+            }
+        std::vector<float> pf(ph.begin(), ph.end());
+        CK(Q->phase64.ensure(ph.size() * sizeof(double)), "cudaMalloc");
+        CK(cudaMemcpy(Q->phase64.p, ph.data(), ph.size() * sizeof(double), cudaMemcpyHostToDevice), "H2D");
+        CK(Q->phase32.ensure(pf.size() * sizeof(float)), "cudaMalloc");
+        CK(cudaMemcpy(Q->phase32.p, pf.data(), pf.size() * sizeof(float), cudaMemcpyHostToDevice), "H2D");
+    }
+    const int id = ctx->next_id++;
+    ctx->qsets[id] = std::move(Q);
+    *qset_id = id;
+    return SMD_OK;
+}
+
+extern "C" int smd_qset_size(smd_ctx *ctx, int qset_id, int *Q)
+{
+    if (!ctx || !Q) return SMD_EINVAL;
+    auto it = ctx->qsets.find(qset_id);
+    if (it == ctx->qsets.end()) return SMD_ENOTFOUND;
+    *Q = it->second->Q;
+    return SMD_OK;
+}
+
+namespace {
+
+struct JobGeom {
+    Lattice *L;
+    QSet *Qs;
+    Plan *tp;
+    int N, Q, n_rec, prec, R, W, waves;
+    size_t elem, celem;
+};
+
+int prepare(smd_ctx *ctx, const smd_job_desc *job, JobGeom &g)
+{
+    if (!job) return fail(ctx, SMD_EINVAL, "job: null");
+    auto li = ctx->lattices.find(job->lattice);
+    if (li == ctx->lattices.end()) return fail(ctx, SMD_ENOTFOUND, "job: unknown lattice");
+    auto qi = ctx->qsets.find(job->qset);
+    if (qi == ctx->qsets.end()) return fail(ctx, SMD_ENOTFOUND, "job: unknown q set");
+    if (qi->second->lattice != job->lattice) return fail(ctx, SMD_EINVAL, "job: q set belongs to another lattice");
+    if (job->n_samples < 1) return fail(ctx, SMD_EINVAL, "job: n_samples < 1");
+    if (job->n_rec < 2) return fail(ctx, SMD_EINVAL, "job: n_rec < 2");
+    if (job->stride < 1) return fail(ctx, SMD_EINVAL, "job: stride < 1");
+    if (!(job->dt > 0.0)) return fail(ctx, SMD_EINVAL, "job: dt must be positive");
+    if (job->precision != SMD_FP64 && job->precision != SMD_FP32)
+        return fail(ctx, SMD_EINVAL, "job: unknown precision");
+    if ((long long)(job->n_rec - 1) * job->stride > 2000000000LL)
+        return fail(ctx, SMD_EINVAL, "job: too many steps");
+    g.L = li->second.get();
+    g.Qs = qi->second.get();
+    g.N = g.L->N;
+    g.Q = g.Qs->Q;
+    g.n_rec = job->n_rec;
+    g.prec = job->precision;
+    if (g.N > rk_max_sites(g.prec))
+        return fail(ctx, SMD_EINVAL, "job: N exceeds the single-CTA capacity of this form");
+    if (g.Qs->use_grid && g.prec == SMD_FP64 && !g.Qs->fp64_ok)
+        return fail(ctx, SMD_EINVAL, "job: grid too large for the FP64 shared-memory transform");
+    g.elem = g.prec == SMD_FP64 ? sizeof(double) : sizeof(float);
+    g.celem = 2 * g.elem;
+    auto pi = ctx->tplans.find(g.n_rec);
+    if (pi == ctx->tplans.end()) {
+        auto P = std::make_unique<Plan>();
+        if (!make_plan(g.n_rec, P->p)) return fail(ctx, SMD_EINVAL, "job: n_rec has a prime factor > 64");
+        CK(upload_twiddles(g.n_rec, P->tw64, P->tw32), "twiddles");
+        pi = ctx->tplans.emplace(g.n_rec, std::move(P)).first;
+    }
+    g.tp = pi->second.get();
+    const int qt = time_fft_qt(g.n_rec, g.prec);
+    const size_t fft_cap = g.prec == SMD_FP64 ? 8192 : 16384;
+    if ((size_t)qt * g.n_rec > fft_cap || time_fft_smem(g.n_rec, qt, g.prec, g.tp->p) > 200 * 1024)
+        return fail(ctx, SMD_EINVAL, "job: n_rec too long for the shared-memory time transform");
+    // chunk of records per RK launch
+    g.R = std::min(g.n_rec, 64);
+    // per-sample device bytes
+    const size_t N = g.N;
+    const size_t per = 2 * 3 * N * sizeof(double) + N + 2 * (size_t)g.R * 3 * N * g.elem +
+                       3 * (size_t)g.n_rec * g.Q * g.celem + (size_t)g.n_rec * sizeof(double) +
+                       5 * sizeof(double);
+    const size_t fixed = 3 * (size_t)g.Q * g.n_rec * sizeof(double) + (64u << 20);
+    if (ctx->budget <= fixed + per) return fail(ctx, SMD_ENOMEM_ADMIT, "job: one sample exceeds the HBM budget");
+    size_t W = (ctx->budget - fixed) / per;
+    W = std::min<size_t>(W, (size_t)job->n_samples);
+    W = std::min<size_t>(W, 65535);
+    g.W = (int)W;
+    g.waves = (job->n_samples + g.W - 1) / g.W;
+    return SMD_OK;
+}
+
+// The pipeline of one job on device buffers; spec/qss sums accumulate.
+int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const double *d_spins0,
+               const double *d_win, double *d_spec_sum, double *d_qss_sum, double *d_final,
+               smd_report *rep)
+{
+    const int N = g.N, Q = g.Q, n_rec = g.n_rec, R = g.R, W = g.W;
+    Lattice &L = *g.L;
+    QSet &Qs = *g.Qs;
+    CK(ctx->state.ensure((size_t)W * 3 * N * sizeof(double)), "cudaMalloc state");
+    CK(ctx->s0.ensure((size_t)W * 3 * N * sizeof(double)), "cudaMalloc s0");
+    CK(ctx->imp.ensure((size_t)W * N), "cudaMalloc imp");
+    for (int b = 0; b < 2; b++)
+        CK(ctx->snap[b].ensure((size_t)W * R * 3 * N * g.elem), "cudaMalloc snap");
+    CK(ctx->series.ensure((size_t)W * 3 * n_rec * Q * g.celem), "cudaMalloc series");
+    CK(ctx->qss.ensure((size_t)W * n_rec * sizeof(double)), "cudaMalloc qss");
+    CK(ctx->stats.ensure((size_t)W * 4 * sizeof(double)), "cudaMalloc stats");
+    CK(ctx->e0.ensure((size_t)W * sizeof(double)), "cudaMalloc e0");
+    CK(ctx->status.ensure(sizeof(int)), "cudaMalloc status");
+    CK(cudaMemsetAsync(ctx->status.p, 0, sizeof(int), ctx->s_rk), "memset");
+    const bool gen = L.lieb_delta || job->imp;
+    std::vector<double> stats_h;
+    double drift_max = 0.0, drift_final = 0.0;
+    double ms_dev = 0.0, ms_rk = 0.0, ms_proj = 0.0, ms_tfft = 0.0;
+    int rk_launches = 0;
+    const int nchunks = (n_rec + R - 1) / R;
+    // event pairs: [0] wave, [1..nchunks] RK launches, then projections, then time FFT
+    const size_t nev = 2 * (size_t)(2 + 2 * nchunks);
+    while (ctx->tev.size() < nev) {
+        cudaEvent_t e;
+        CK(cudaEventCreate(&e), "event");
+        ctx->tev.push_back(e);
+    }
+    auto ev = [&](size_t k) { return ctx->tev[k]; };
+    auto elapsed = [&](size_t a, size_t b) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev(a), ev(b));
+        return (double)ms;
+    };
+
+    for (int w = 0; w < g.waves; w++) {
+        const int s_begin = w * W;
+        const int Ww = std::min(W, job->n_samples - s_begin);
+        CK(cudaEventRecord(ev(0), ctx->s_rk), "event");
+        CK(launch_aos_to_soa(d_spins0 + (size_t)s_begin * N * 3, ctx->state.as<double>(), Ww, N,
+                             ctx->s_rk), "aos_to_soa");
+        ctx->launches++;
+        CK(cudaMemcpyAsync(ctx->s0.p, ctx->state.p, (size_t)Ww * 3 * N * sizeof(double),
+                           cudaMemcpyDeviceToDevice, ctx->s_rk), "D2D");
+        if (job->imp) {
+            std::vector<uint8_t> ib((size_t)Ww * N);
+            for (size_t e = 0; e < ib.size(); e++) ib[e] = job->imp[(size_t)s_begin * N + e] ? 1 : 0;
+            CK(cudaMemcpyAsync(ctx->imp.p, ib.data(), ib.size(), cudaMemcpyHostToDevice, ctx->s_rk),
+               "H2D imp");
+            CK(cudaStreamSynchronize(ctx->s_rk), "sync");
+        }
+        // the proj stream must not overwrite series of the previous wave
+        // before its time transform finished: both run on s_proj in order.
+        for (int c = 0; c < nchunks; c++) {
+            const int b = c & 1;
+            const int rb = c * R, re = std::min(n_rec, rb + R);
+            if (c >= 2) CK(cudaStreamWaitEvent(ctx->s_rk, ctx->ev_proj[b], 0), "wait");
+            RKJob J{};
+            J.n_samples = Ww;
+            J.dt = job->dt;
+            J.stride = job->stride;
+            J.rec_begin = rb;
+            J.rec_end = re;
+            J.n_rec = n_rec;
+            J.fix_every = job->fix_every < 1 ? 1 : job->fix_every;
+            J.state = ctx->state.as<double>();
+            J.s0 = ctx->s0.as<double>();
+            J.e0 = ctx->e0.as<double>();
+            J.imp = job->imp ? ctx->imp.as<uint8_t>() : nullptr;
+            J.snap = ctx->snap[b].p;
+            J.snap_R = R;
+            J.qss = ctx->qss.as<double>();
+            J.stats = ctx->stats.as<double>();
+            J.status = ctx->status.as<int>();
+            CK(cudaEventRecord(ev(2 + 2 * c), ctx->s_rk), "event");
+            CK(launch_rk(L.dev, J, g.prec, gen, ctx->s_rk), "rk kernel");
+            CK(cudaEventRecord(ev(3 + 2 * c), ctx->s_rk), "event");
+            ctx->launches++;
+            rk_launches++;
+            CK(cudaEventRecord(ctx->ev_rk[b], ctx->s_rk), "event");
+            CK(cudaStreamWaitEvent(ctx->s_proj, ctx->ev_rk[b], 0), "wait");
+            CK(cudaEventRecord(ev(2 + 2 * nchunks + 2 * c), ctx->s_proj), "event");
+            if (Qs.use_grid) {
+                const double scale = std::sqrt(1.0 / ((double)Qs.G * Qs.G));   // subrouts.cpp:8343
+                CK(launch_grid_proj(ctx->snap[b].p, g.prec, N, Ww, R, re - rb, rb, n_rec,
+                                    L.grid_map.as<int>(), Qs.gplan,
+                                    g.prec == SMD_FP64 ? Qs.tw64.p : Qs.tw32.p, scale,
+                                    ctx->series.p, Q, ctx->s_proj), "grid projection");
+                ctx->launches++;
+            }
+            if (Qs.n_list > 0) {
+                CK(launch_list_proj_simt(ctx->snap[b].p, g.prec, Ww, R, re - rb, N, rb, n_rec,
+                                         g.prec == SMD_FP64 ? Qs.phase64.p : Qs.phase32.p,
+                                         Qs.n_list, ctx->series.p, Q, Qs.G * Qs.G, ctx->s_proj),
+                   "list projection");
+                ctx->launches++;
+            }
+            CK(cudaEventRecord(ev(3 + 2 * nchunks + 2 * c), ctx->s_proj), "event");
+            CK(cudaEventRecord(ctx->ev_proj[b], ctx->s_proj), "event");
+        }
+        CK(cudaEventRecord(ev(nev - 2), ctx->s_proj), "event");
+        CK(launch_time_fft(ctx->series.p, g.prec, Ww, Q, g.tp->p,
+                           g.prec == SMD_FP64 ? g.tp->tw64.p : g.tp->tw32.p, d_win, d_spec_sum,
+                           ctx->s_proj), "time fft");
+        CK(cudaEventRecord(ev(nev - 1), ctx->s_proj), "event");
+        ctx->launches++;
+        CK(cudaStreamWaitEvent(ctx->s_proj, ctx->ev_rk[(nchunks - 1) & 1], 0), "wait");
+        CK(launch_sum_rows(ctx->qss.as<double>(), Ww, n_rec, d_qss_sum, ctx->s_proj), "qss");
+        ctx->launches++;
+        if (d_final) {
+            CK(launch_soa_to_aos(ctx->state.as<double>(), d_final + (size_t)s_begin * N * 3, Ww, N,
+                                 ctx->s_proj), "soa_to_aos");
+            ctx->launches++;
+        }
+        CK(cudaEventRecord(ev(1), ctx->s_proj), "event");
+        stats_h.resize((size_t)Ww * 4);
+        CK(cudaMemcpyAsync(stats_h.data(), ctx->stats.p, stats_h.size() * sizeof(double),
+                           cudaMemcpyDeviceToHost, ctx->s_proj), "D2H stats");
+        // before the next wave overwrites state / series / qss
+        CK(cudaStreamSynchronize(ctx->s_proj), "sync");
+        CK(cudaStreamSynchronize(ctx->s_rk), "sync");
+        ms_dev += elapsed(0, 1);
+        for (int c = 0; c < nchunks; c++) {
+            ms_rk += elapsed(2 + 2 * c, 3 + 2 * c);
+            ms_proj += elapsed(2 + 2 * nchunks + 2 * c, 3 + 2 * nchunks + 2 * c);
+        }
+        ms_tfft += elapsed(nev - 2, nev - 1);
+        for (int s = 0; s < Ww; s++) {
+            drift_max = std::max(drift_max, stats_h[s * 4 + 0] / N);
+            drift_final = std::max(drift_final, std::fabs(stats_h[s * 4 + 1] - stats_h[s * 4 + 2]) / N);
+        }
+    }
+    int st = 0;
+    CK(cudaMemcpy(&st, ctx->status.p, sizeof(int), cudaMemcpyDeviceToHost), "D2H status");
+    if (rep) {
+        rep->drift_max = drift_max;
+        rep->drift_final = drift_final;
+        rep->waves = g.waves;
+        rep->ms_device = ms_dev;
+        rep->ms_rk = ms_rk;
+        rep->ms_proj = ms_proj;
+        rep->ms_tfft = ms_tfft;
+        rep->rk_launches = rk_launches;
+        rep->site_steps = (double)N * (double)(n_rec - 1) * job->stride * job->n_samples;
+    }
+    if (st) return fail(ctx, SMD_ECUDA, "a sample reached a zero correction denominator (sigma = 0)");
+    return SMD_OK;
+}
+
+}  // namespace
+
+extern "C" int smd_run_device(smd_ctx *ctx, const smd_job_desc *job, const double *d_spins0,
+                              const double *d_window, double *d_spec_sum, double *d_qss_sum,
+                              double *d_final, smd_report *rep)
+{
+    if (!ctx || !job || !d_spins0 || !d_window || !d_spec_sum || !d_qss_sum) return SMD_EINVAL;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    JobGeom g;
+    int rc = prepare(ctx, job, g);
+    if (rc) return rc;
+    ctx->launches = 0;
+    auto w0 = std::chrono::steady_clock::now();
+    rc = run_device(ctx, job, g, d_spins0, d_window, d_spec_sum, d_qss_sum, d_final, rep);
+    auto w1 = std::chrono::steady_clock::now();
+    if (rep) {
+        rep->ms_total = std::chrono::duration<double, std::milli>(w1 - w0).count();
+        rep->ms_h2d = rep->ms_d2h = 0.0;
+        rep->kernel_launches = ctx->launches;
+    }
+    return rc;
+}
+
+extern "C" int smd_run(smd_ctx *ctx, const smd_job_desc *job, const double *spins0,
+                       const double *window, double *spec_out, double *qss_out, double *final_out,
+                       smd_report *rep)
+{
+    if (!ctx || !job || !spins0 || !window || !spec_out || !qss_out) return SMD_EINVAL;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    JobGeom g;
+    int rc = prepare(ctx, job, g);
+    if (rc) return rc;
+    ctx->launches = 0;
+    const size_t S = job->n_samples, N = g.N, Q = g.Q, n = g.n_rec;
+    const size_t in_b = S * N * 3 * sizeof(double);
+    const size_t acc_b = 3 * Q * n * sizeof(double);
+    const size_t out_b = (final_out ? in_b : 0);
+    CK(ctx->in_tmp.ensure(in_b + n * sizeof(double)), "cudaMalloc");
+    CK(ctx->acc_tmp.ensure(acc_b + n * sizeof(double)), "cudaMalloc");
+    if (out_b) CK(ctx->out_tmp.ensure(out_b), "cudaMalloc");
+    double *d_in = ctx->in_tmp.as<double>();
+    double *d_win = d_in + S * N * 3;
+    double *d_acc = ctx->acc_tmp.as<double>();
+    double *d_q = d_acc + 3 * Q * n;
+    auto w0 = std::chrono::steady_clock::now();
+    CK(cudaMemcpyAsync(d_in, spins0, in_b, cudaMemcpyHostToDevice, ctx->s_rk), "H2D spins");
+    CK(cudaMemcpyAsync(d_win, window, n * sizeof(double), cudaMemcpyHostToDevice, ctx->s_rk), "H2D window");
+    CK(cudaMemsetAsync(d_acc, 0, acc_b + n * sizeof(double), ctx->s_rk), "memset");
+    CK(cudaStreamSynchronize(ctx->s_rk), "sync");
+    auto w1 = std::chrono::steady_clock::now();
+    rc = run_device(ctx, job, g, d_in, d_win, d_acc, d_q, out_b ? ctx->out_tmp.as<double>() : nullptr,
+                    rep);
+    if (rc) return rc;
+    auto w2 = std::chrono::steady_clock::now();
+    CK(cudaMemcpy(spec_out, d_acc, acc_b, cudaMemcpyDeviceToHost), "D2H spec");
+    CK(cudaMemcpy(qss_out, d_q, n * sizeof(double), cudaMemcpyDeviceToHost), "D2H qss");
+    if (out_b) CK(cudaMemcpy(final_out, ctx->out_tmp.p, out_b, cudaMemcpyDeviceToHost), "D2H final");
+    // average over samples, as the reference's fc = 1 / evoCnt (smd_code.cpp:3596-3611)
+    const double fc = 1.0 / (double)S;
+    for (size_t e = 0; e < 3 * Q * n; e++) spec_out[e] = fc * spec_out[e];
+    for (size_t t = 0; t < n; t++) qss_out[t] = fc * qss_out[t];
+    auto w3 = std::chrono::steady_clock::now();
+    if (rep) {
+        rep->ms_h2d = std::chrono::duration<double, std::milli>(w1 - w0).count();
+        rep->ms_d2h = std::chrono::duration<double, std::milli>(w3 - w2).count();
+        rep->ms_total = std::chrono::duration<double, std::milli>(w3 - w0).count();
+        rep->kernel_launches = ctx->launches;
+    }
+    return SMD_OK;
+}
+
+extern "C" int smd_dyn_spectrum_ref(smd_ctx *ctx, int lattice_id, int qset_id, double dtm, int ntm,
+                                    const double *tWinVec, double *spinField, const int *imp,
+                                    double *SqxWVec, double *SqyWVec, double *SqzWVec,
+                                    double *qSStVec)
+{
+    if (!ctx || !tWinVec || !spinField || !SqxWVec || !SqyWVec || !SqzWVec || !qSStVec)
+        return SMD_EINVAL;
+    smd_job_desc job{};
+    job.lattice = lattice_id;
+    job.qset = qset_id;
+    job.n_samples = 1;
+    job.dt = dtm;
+    job.n_rec = ntm;
+    job.stride = 1;
+    job.precision = SMD_FP64;
+    job.fix_every = 1;
+    job.imp = imp;
+    int Q = 0;
+    int rc = smd_qset_size(ctx, qset_id, &Q);
+    if (rc) return rc;
+    std::vector<double> spec((size_t)3 * Q * ntm), fin;
+    auto li = ctx->lattices.find(lattice_id);
+    if (li == ctx->lattices.end()) return SMD_ENOTFOUND;
+    fin.resize((size_t)li->second->N * 3);
+    rc = smd_run(ctx, &job, spinField, tWinVec, spec.data(), qSStVec, fin.data(), nullptr);
+    if (rc) return rc;
+    const size_t blk = (size_t)Q * ntm;
+    std::memcpy(SqxWVec, spec.data(), blk * sizeof(double));
+    std::memcpy(SqyWVec, spec.data() + blk, blk * sizeof(double));
+    std::memcpy(SqzWVec, spec.data() + 2 * blk, blk * sizeof(double));
+    std::memcpy(spinField, fin.data(), fin.size() * sizeof(double));
+    return SMD_OK;
+}
+
+extern "C" int smd_evolve(smd_ctx *ctx, int lattice_id, int precision, int n_samples, double dt,
+                          int nsteps, int fix_every, const int *imp, double *spins, smd_report *rep)
+{
+    if (!ctx || !spins || nsteps < 1) return SMD_EINVAL;
+    auto li = ctx->lattices.find(lattice_id);
+    if (li == ctx->lattices.end()) return fail(ctx, SMD_ENOTFOUND, "evolve: unknown lattice");
+    // a q set of one list point keeps the pipeline shape; two records
+    // (start and end) with stride nsteps give the final state
+    int qid = -1;
+    double q0[2] = {0.0, 0.0};
+    Lattice &L = *li->second;
+    std::vector<double> fake_pos;
+    if (L.pos.empty()) L.pos.assign(2 * (size_t)L.N, 0.0);
+    int rc = smd_qset_upload(ctx, lattice_id, 0, 1, q0, 1.0, &qid);
+    if (rc) return rc;
+    smd_job_desc job{};
+    job.lattice = lattice_id;
+    job.qset = qid;
+    job.n_samples = n_samples;
+    job.dt = dt;
+    job.n_rec = 2;
+    job.stride = nsteps;
+    job.precision = precision;
+    job.fix_every = fix_every;
+    job.imp = imp;
+    std::vector<double> spec(3 * 2), qss(2), win(2, 1.0);
+    if (precision == SMD_FP32) {
+        // the FP32 form has no list projection yet; use the grid if present
+        ctx->qsets.erase(qid);
+        rc = smd_qset_upload(ctx, lattice_id, 1, 0, nullptr, 1.0, &qid);
+        if (rc) return rc;
+        int Q = 0;
+        smd_qset_size(ctx, qid, &Q);
+        spec.assign((size_t)3 * Q * 2, 0.0);
+        job.qset = qid;
+    }
+    rc = smd_run(ctx, &job, spins, win.data(), spec.data(), qss.data(), spins, rep);
+    ctx->qsets.erase(qid);
+    return rc;
+}
+
+// ------------------------------------------------------------- serving
+// (filled in by serve.cu)
+
+extern "C" int smd_lattice_sites(smd_ctx *ctx, int lattice_id, int *N)
+{
+    if (!ctx || !N) return SMD_EINVAL;
+    auto it = ctx->lattices.find(lattice_id);
+    if (it == ctx->lattices.end()) return SMD_ENOTFOUND;
+    *N = it->second->N;
+    return SMD_OK;
+}

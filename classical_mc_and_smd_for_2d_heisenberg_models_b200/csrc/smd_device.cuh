@@ -1,0 +1,105 @@
+// smd_device.cuh -- device-side data layout and helpers shared by the SMD
+// kernels.
+//
+// HBM layout (per sample wave of W samples):
+//   state    double [W][3][N]   FP64 spins, one SoA row per component
+//   s0       double [W][3][N]   initial spins (for the autocorrelation)
+//   imp      uint8  [W][N]      impurity flags (disordered lattices only)
+//   snap     T      [W][R][3][N] spin snapshots of the R records of a chunk
+//   series   cT     [W][3][n_rec][Q] S(q,t), q fastest
+//   acc      double [3][Q][n_rec] sum over samples of |S(q,w)|^2
+//   qss      double [W][n_rec]  per-sample spin autocorrelation
+// Neighbour tables are ELL, [ztot][N] (shell s occupies rows zoff[s] ..
+// zoff[s] + zn[s] - 1), so that a warp reading the k-th neighbour of 32
+// consecutive sites issues one coalesced 128-byte load.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace smd {
+
+struct LatticeDev {
+    int N;
+    int zn[3];
+    int zoff[3];
+    int ztot;
+    const int *nbr;          // ELL [ztot][N]
+    int shell_on[3];
+    double J[3][2][2];
+    double lam[3][3];
+    double coef[3][3];       // J[s][0][0] * lam[s][.]
+    int lieb_delta_on;
+    double j2_delta;
+    double h;
+    float Jf[3][2][2], lamf[3][3], coeff[3][3], j2_deltaf, hf;
+    int energy_from_field;   // E = 1/2 sum_i (S_i . h_i - h S_i^z) holds
+    int nbonds;              // explicit bond list (used when the identity fails)
+    const int4 *bonds;       // (i, j, shell, 0)
+};
+
+struct RKJob {
+    int n_samples;
+    double dt;
+    int stride;
+    int rec_begin, rec_end;  // records written by this launch
+    int n_rec;
+    int fix_every;
+    double *state;           // [W][3][N]
+    const double *s0;        // [W][3][N]
+    double *e0;              // [W]
+    const uint8_t *imp;      // [W][N] or null
+    void *snap;              // [W][R][3][N] of the snapshot type
+    int snap_R;
+    double *qss;             // [W][n_rec]
+    double *stats;           // [W][4]: max drift, last E, E0, sigma_min
+    int *status;             // nonzero after a numerical failure
+};
+
+enum { kStatusOK = 0, kStatusBadSigma = 1 };
+
+// Mixed-radix factorisation of a transform length (product of radix = n).
+struct FFTPlan {
+    int n;
+    int nst;
+    int radix[16];
+};
+
+template <typename T>
+struct cplx {
+    T x, y;
+};
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block-wide sum of NV doubles; every thread receives the totals.  red holds
+// two slots of [32][NV]; alternating slots lets consecutive reductions run
+// with a single barrier each.  Summation order is fixed, so results are
+// deterministic run to run.
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double *red, int &slot)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; k++) v[k] = warp_sum(v[k]);
+    double *r = red + slot * 32 * NV;
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) r[warp * NV + k] = v[k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+        double x = (lane < nw) ? r[lane * NV + k] : 0.0;
+        v[k] = warp_sum(x);
+    }
+    slot ^= 1;
+}
+
+}  // namespace smd

@@ -1,0 +1,30 @@
+// smd_launch.h -- host-side declarations of the kernel launchers.
+#pragma once
+
+#include "smd_device.cuh"
+
+namespace smd {
+
+size_t rk_smem_bytes(int N, int precision);
+int rk_threads(int N, int precision);
+int rk_max_sites(int precision);
+cudaError_t launch_rk(const LatticeDev &L, const RKJob &J, int precision, bool gen,
+                      cudaStream_t st);
+
+size_t grid_proj_smem(int G, int precision, const FFTPlan &p);
+cudaError_t launch_grid_proj(const void *snap, int precision, int N, int W, int R, int nrec_chunk,
+                             int rec_begin, int n_rec_total, const int *grid_map,
+                             const FFTPlan &plan, const void *tw, double scale, void *series,
+                             int Q, cudaStream_t st);
+cudaError_t launch_list_proj_simt(const void *snap, int precision, int W, int R, int nrec_chunk,
+                                  int N, int rec_begin, int n_rec_total, const void *P, int Lq,
+                                  void *series, int Q, int qoff, cudaStream_t st);
+int time_fft_qt(int n, int precision);
+size_t time_fft_smem(int n, int qt, int precision, const FFTPlan &p);
+cudaError_t launch_time_fft(const void *series, int precision, int W, int Q, const FFTPlan &plan,
+                            const void *tw, const double *win, double *acc, cudaStream_t st);
+cudaError_t launch_aos_to_soa(const double *in, double *out, int W, int N, cudaStream_t st);
+cudaError_t launch_soa_to_aos(const double *in, double *out, int W, int N, cudaStream_t st);
+cudaError_t launch_sum_rows(const double *rows, int W, int n, double *out, cudaStream_t st);
+
+}  // namespace smd

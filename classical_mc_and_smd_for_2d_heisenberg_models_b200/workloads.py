@@ -1,0 +1,115 @@
+"""Synthetic SMD workloads with the shapes of the benchmark configurations.
+
+There is no public data set for this path: seeded synthetic samples in the
+reference's sample-file format stand in for MC output (ordered states with
+Gaussian tangent tilts).  Every workload is a settings object, a sample
+count, the ordered state and tilt, the record stride and length, the
+precision form, and the q points.
+
+  c1  square L=16 (N=256), J1=1 J2=0.6, 8 samples, stripe +x with 0.2 rad
+      tilts, FP64 plain, dt=0.01, stride 4, 1024 records (512 positive
+      frequencies), full 16 x 16 grid
+  c2  triangular L=48 (N=2304), J2=0.12, 64 samples, 120-degree state with
+      0.15 rad tilts, FP32 precision form, dt=0.02, stride 4, 4096 records
+      (2048 positive frequencies), FP64 correction every 16 steps,
+      48 x 48 grid + 512-point Gamma-K-M-Gamma path
+  c4  square L=128 (N=16384), J2=0.55 J3=0.1 lambda=0.9 h=0.3, 5% vacancies,
+      512 samples, stripe with 0.1 rad tilts, FP32, dt=0.01, stride 8,
+      4096 records, 128 x 128 grid + 1024-point path
+The number of RK steps of a job is (records - 1) * stride.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import Optional
+
+import numpy as np
+
+from ._lib import SMD_FP32, SMD_FP64
+from .settings import SMDSettings
+
+
+@dataclasses.dataclass
+class Workload:
+    name: str
+    settings: SMDSettings
+    n_samples: int
+    state: str
+    sigma: float
+    stride: int
+    n_rec: int
+    precision: int
+    fix_every: int
+    qpath_points: int
+    seed: int
+    window: str = "hann1"
+
+    @property
+    def steps(self) -> int:
+        return (self.n_rec - 1) * self.stride
+
+    def describe(self) -> str:
+        s = self.settings
+        return (f"{self.name}: {s.geom} L={s.L} N={s.N}, J2={s.J2} JX={s.JX} h={s.h} "
+                f"vac={s.imp_ratio}, {self.n_samples} samples, {self.steps} RK4 steps "
+                f"(stride {self.stride}, {self.n_rec} records), "
+                f"{'FP64 plain' if self.precision == SMD_FP64 else 'FP32 precision form'}, "
+                f"{s.G}x{s.G} grid + {self.qpath_points}-point path")
+
+
+def path_points(geom: str, n: int) -> np.ndarray:
+    """n points along a closed high-symmetry path, uniform in arc length.
+
+    C3 lattices: Gamma -> K -> M -> Gamma with K = (4 pi / 3, 0) (the
+    reference's Qvec0, Codes_Folder/subrouts.cpp:523-530) and M = (pi, pi/sqrt3);
+    square-like lattices: Gamma -> X -> M -> Gamma with X = (pi, 0), M = (pi, pi).
+    """
+    if geom in ("square", "lieb"):
+        corners = [(0.0, 0.0), (math.pi, 0.0), (math.pi, math.pi), (0.0, 0.0)]
+    else:
+        corners = [(0.0, 0.0), (4.0 * math.pi / 3.0, 0.0),
+                   (math.pi, math.pi / math.sqrt(3.0)), (0.0, 0.0)]
+    c = np.array(corners)
+    seg = np.linalg.norm(np.diff(c, axis=0), axis=1)
+    total = seg.sum()
+    t = np.arange(n) * total / n
+    out = np.zeros((n, 2))
+    start = np.concatenate([[0.0], np.cumsum(seg)])
+    for k in range(n):
+        s = min(np.searchsorted(start, t[k], side="right") - 1, len(seg) - 1)
+        f = (t[k] - start[s]) / seg[s]
+        out[k] = c[s] + f * (c[s + 1] - c[s])
+    return out
+
+
+def c1() -> Workload:
+    s = SMDSettings(geom="square", L=16, J1=1.0, J2=0.6, dtm=0.01, ntm=1024, NMeas=8000)
+    return Workload("c1", s, 8, "stripe", 0.2, 4, 1024, SMD_FP64, 1, 0, 0x5eed01)
+
+
+def c2(n_samples: int = 64) -> Workload:
+    s = SMDSettings(geom="triang", L=48, J1=1.0, J2=0.12, dtm=0.02, ntm=4096,
+                    NMeas=1000 * max(2, n_samples))
+    return Workload("c2", s, n_samples, "q120", 0.15, 4, 4096, SMD_FP32, 16, 512, 0x5eed02)
+
+
+def c4(n_samples: int = 512) -> Workload:
+    s = SMDSettings(geom="square", L=128, J1=1.0, J2=0.55, JX=0.1, zlamb1=0.9, zlamb2=0.9,
+                    h=0.3, imp_ratio=0.05, dtm=0.01, ntm=4096, NMeas=1000 * n_samples,
+                    outTag="Htag")
+    return Workload("c4", s, n_samples, "stripe", 0.1, 8, 4096, SMD_FP32, 16, 1024, 0x5eed04)
+
+
+WORKLOADS = {"c1": c1, "c2": c2, "c4": c4}
+
+
+def make_inputs(w: Workload, rank: int = 0):
+    """Samples (and per-sample impurity maps) for one rank."""
+    from . import samples as smp
+    spins, imp = smp.make_samples(w.settings, w.n_samples, w.state, w.sigma, w.seed + 7919 * rank)
+    imp_per_sample = None
+    if imp is not None:
+        P = w.settings.pack_size
+        imp_per_sample = np.stack([imp[k // P] for k in range(w.n_samples)])
+    return spins, imp_per_sample

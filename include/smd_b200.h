@@ -1,0 +1,233 @@
+/*
+ * smd_b200.h -- C ABI of the B200 semiclassical spin-dynamics (SMD) library.
+ *
+ * The library replaces the reference's SMD hot path, the per-sample function
+ *
+ *   void get_dynSpectrum(int procNum, double *tWinVec, double **spinField,
+ *                        double **SqxWVec, double **SqyWVec,
+ *                        double **SqzWVec, double *qSStVec)
+ *   (Codes_Folder/subrouts.cpp:11547-12149)
+ *
+ * together with the sample loop and accumulation of its caller
+ * (Codes_Folder/smd_code.cpp:3079-3291, 3596-3611), with hand-written sm_100a
+ * kernels.  Everything the reference reads from process globals (lattice
+ * tables, couplings, lambda vectors, field, ntm, dtm, the DFT grid map; see
+ * Codes_Folder/subrouts.cpp:65-775) is passed explicitly.
+ *
+ * Conventions
+ *   - plain C types only; host memory belongs to the caller, device memory to
+ *     the context;
+ *   - every entry point returns an smd_status; smd_last_error() describes the
+ *     last failure of a context;
+ *   - one context per host thread; a context is not re-entrant;
+ *   - spins are [site][3] doubles in the reference's site order, exactly as
+ *     the reference's spinField rows and sample files hold them;
+ *   - spectra are [3][Q][n_rec] doubles (component, q, frequency bin), the
+ *     reference's SqxWVec/SqyWVec/SqzWVec rows stacked by component; grid q
+ *     come first in the reference's k = i * Gsz + j order
+ *     (Codes_Folder/subrouts.cpp:8421-8431), then the list q.
+ */
+#ifndef SMD_B200_H
+#define SMD_B200_H
+
+#include <stddef.h>
+
+#if defined(__GNUC__)
+#define SMD_API __attribute__((visibility("default")))
+#else
+#define SMD_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    SMD_OK = 0,
+    SMD_EINVAL = 1,        /* invalid argument or unsupported size */
+    SMD_ENOMEM_ADMIT = 2,  /* job does not fit the context's HBM budget */
+    SMD_ECUDA = 3,         /* CUDA runtime or kernel error */
+    SMD_ETIMEOUT = 4,      /* a bounded wait expired */
+    SMD_ECANCELLED = 5,    /* job cancelled before completion */
+    SMD_ENOTFOUND = 6,     /* unknown lattice, q-set or job id */
+    SMD_EBUSY = 7          /* job not finished yet (smd_poll) */
+} smd_status;
+
+typedef enum {
+    SMD_FP64 = 0,          /* plain form: every step in FP64, correction each step */
+    SMD_FP32 = 1           /* precision form: FP32 RK4 stages, FP64 master spins,
+                              renormalisation and energy correction */
+} smd_precision;
+
+typedef enum {
+    SMD_SQUARE = 0, SMD_TRIANG = 1, SMD_HEXAGN = 2, SMD_KAGOME = 3, SMD_LIEB = 4
+} smd_geometry;
+
+typedef struct smd_ctx smd_ctx;
+
+typedef struct {
+    int device;            /* CUDA device ordinal */
+    size_t hbm_budget;     /* bytes the context may hold for job state; 0 = 85% of free */
+} smd_device_opts;
+
+/* ------------------------------------------------------------ context */
+
+SMD_API int smd_ctx_create(const smd_device_opts *opts, smd_ctx **out);
+SMD_API int smd_ctx_destroy(smd_ctx *ctx);
+SMD_API const char *smd_last_error(const smd_ctx *ctx);
+SMD_API const char *smd_version(void);
+
+/* -------------------------------------------------- host lattice tables */
+
+/* Geometry constants of convert_inputs2data
+ * (Codes_Folder/subrouts.cpp:1028-1067, 1141-1154): N = nSubs L^2,
+ * G = gridFac L, zn = (Zn1, Zn2, ZnX).  Also applies the reference's size
+ * rules (L even; L a multiple of 3 for the C3 lattices). */
+SMD_API int smd_geometry_info(int geom, int L, int *N, int *G, int *nsubs, int zn[3]);
+
+/* Site positions, DFT-grid map and neighbour tables in the reference's exact
+ * order, replacing make_rvecList (Codes_Folder/subrouts.cpp:2714-2962) and
+ * make_nborsTable (Codes_Folder/subrouts.cpp:2983-3316).  Built in O(N) from
+ * cell neighbourhoods instead of the reference's O(N^2) search.
+ * rvec[N][2], grid_map[G*G], nb1[N][zn0], nb2[N][zn1], nbx[N][zn2]. */
+SMD_API int smd_build_lattice(int geom, int L, double *rvec, int *grid_map, int *nb1,
+                      int *nb2, int *nbx);
+
+/* Bond list of make_bondList (Codes_Folder/subrouts.cpp:3426-3570).
+ * bonds[max_bonds][2]; nbonds = {total, NN, NNN, Xth}. */
+SMD_API int smd_build_bonds(int N, const int zn[3], const int *nb1, const int *nb2,
+                    const int *nbx, int j2_on, int jx_on, int *bonds,
+                    int max_bonds, int nbonds[4]);
+
+/* Temporal windows of Codes_Folder/aux_code.cpp:249-435, selected by the
+ * names of Codes_Folder/smd_code.cpp:2825-2894 (nowin gauss ntall black
+ * flatw lancz sincw hann1 hann2 hann3). */
+SMD_API int smd_window(const char *name, int n, double *out);
+
+/* ------------------------------------------------------ device objects */
+
+/* Model on one lattice: what get_localField (Codes_Folder/subrouts.cpp:
+ * 4465-4570) and get_energyValue (Codes_Folder/subrouts.cpp:5181-5302) read
+ * from globals. */
+typedef struct {
+    int N;                 /* Ns */
+    int zn[3];             /* Zn1, Zn2, ZnX */
+    const int *nbr[3];     /* nbors1/2/X as [N][zn[s]]; entries < 0 are ghosts */
+    int shell_on[3];       /* 1, J2_ON, JX_ON */
+    double J[3][2][2];     /* J1Mat, J2Mat, JXMat [a_i][a_j] */
+    double lambda[3][3];   /* lambdaVec1..3 */
+    int lieb_delta_on;     /* J2ab_ON */
+    double j2_delta;       /* J2_delta */
+    double h;              /* extH along z */
+    int nbonds[3];         /* Nb1, Nb2, NbX */
+    const int *bonds;      /* bondList as [Nb][2] */
+    int G;                 /* Gsz; 0 = no DFT grid */
+    const int *grid_map;   /* gridMap [G*G], -1 = empty grid point */
+    const double *pos;     /* [N][2] site positions for list-q projection */
+} smd_lattice_desc;
+
+SMD_API int smd_lattice_upload(smd_ctx *ctx, const smd_lattice_desc *desc, int *lattice_id);
+SMD_API int smd_lattice_free(smd_ctx *ctx, int lattice_id);
+
+/* q set: the lattice's G x G grid (use_grid = 1) followed by n_list
+ * arbitrary points q = qlist[l] ([n_list][2]).  List points use the direct
+ * sum of get_qct_SqData (Codes_Folder/subrouts.cpp:8460-8525):
+ * list_scale * sum_k S_k exp(-i q . pos_k). */
+SMD_API int smd_qset_upload(smd_ctx *ctx, int lattice_id, int use_grid, int n_list,
+                    const double *qlist, double list_scale, int *qset_id);
+SMD_API int smd_qset_size(smd_ctx *ctx, int qset_id, int *Q);
+SMD_API int smd_lattice_sites(smd_ctx *ctx, int lattice_id, int *N);
+
+/* ----------------------------------------------------------------- jobs */
+
+typedef struct {
+    int lattice;           /* lattice id */
+    int qset;              /* q-set id (on the same lattice) */
+    int n_samples;         /* samples in spins0 */
+    double dt;             /* dtm */
+    int n_rec;             /* records = time-FFT length (the reference's ntm) */
+    int stride;            /* RK steps between records (reference: 1) */
+    int precision;         /* smd_precision */
+    int fix_every;         /* energy-correction period in steps (reference: 1) */
+    const int *imp;        /* [n_samples][N] impurity flags, or NULL */
+} smd_job_desc;
+
+typedef struct {
+    double ms_total;       /* wall time of the call on the device stream */
+    double ms_h2d, ms_d2h; /* host <-> device copies inside the call */
+    double site_steps;     /* N * RK steps * samples */
+    double drift_max;      /* max over samples and checked steps of |E - E0| / N */
+    double drift_final;    /* max over samples of |E(final) - E0| / N */
+    int waves;             /* sample waves the job was split into */
+    int kernel_launches;   /* kernels launched by the call */
+    double ms_device;      /* device time of the pipeline (CUDA events, all waves) */
+    double ms_rk;          /* summed duration of the RK kernel launches */
+    double ms_proj;        /* summed duration of the projection launches */
+    double ms_tfft;        /* summed duration of the time-transform launches */
+    int rk_launches;       /* RK kernel launches */
+} smd_report;
+
+/* Run a job end to end from host buffers.
+ * spins0      [n_samples][N][3] initial spins (host)
+ * window      [n_rec] temporal window (host)
+ * spec_out    [3][Q][n_rec] sample average of |S(q,w)|^2 (host), the
+ *             reference's CMT_Sq*WVec / evoCnt (Codes_Folder/smd_code.cpp:
+ *             3596-3611)
+ * qss_out     [n_rec] sample average of the spin autocorrelation (host)
+ * final_out   [n_samples][N][3] final spins (host) or NULL */
+SMD_API int smd_run(smd_ctx *ctx, const smd_job_desc *job, const double *spins0,
+            const double *window, double *spec_out, double *qss_out,
+            double *final_out, smd_report *rep);
+
+/* Same job with every buffer already in device memory (pointers from
+ * cudaMalloc on the context's device).  Outputs are sample SUMS, not
+ * averages: spec_sum[3][Q][n_rec] and qss_sum[n_rec] are accumulated into
+ * (caller zeroes them), so several calls can share one accumulator. */
+SMD_API int smd_run_device(smd_ctx *ctx, const smd_job_desc *job, const double *d_spins0,
+                   const double *d_window, double *d_spec_sum, double *d_qss_sum,
+                   double *d_final, smd_report *rep);
+
+/* Reference-equivalent single sample: the data of get_dynSpectrum with flat
+ * arrays.  One RK step per record (stride 1), correction every step, FP64.
+ * spinField [N][3] is updated to the final state; SqxWVec, SqyWVec,
+ * SqzWVec are [Q][ntm] each; qSStVec [ntm]. */
+SMD_API int smd_dyn_spectrum_ref(smd_ctx *ctx, int lattice_id, int qset_id, double dtm,
+                         int ntm, const double *tWinVec, double *spinField,
+                         const int *imp, double *SqxWVec, double *SqyWVec,
+                         double *SqzWVec, double *qSStVec);
+
+/* RK evolution only (no projection): nsteps steps of the chosen form,
+ * spins [n_samples][N][3] updated in place (host). */
+SMD_API int smd_evolve(smd_ctx *ctx, int lattice_id, int precision, int n_samples,
+               double dt, int nsteps, int fix_every, const int *imp,
+               double *spins, smd_report *rep);
+
+/* ------------------------------------------------------------- serving */
+
+/* Continuous batching: a submitted job is admitted by HBM footprint when
+ * memory frees up, its samples are interleaved with other running jobs on
+ * the device, and its result is the same as smd_run of the job alone.
+ * Inputs are copied at submit; outputs go to the host buffers given at
+ * submit, valid once smd_poll returns SMD_OK. */
+SMD_API int smd_submit(smd_ctx *ctx, const smd_job_desc *job, const double *spins0,
+               const double *window, double *spec_out, double *qss_out,
+               long long *job_id);
+SMD_API int smd_poll(smd_ctx *ctx, long long job_id, double *latency_ms);
+SMD_API int smd_wait(smd_ctx *ctx, long long job_id, double timeout_ms, double *latency_ms);
+SMD_API int smd_cancel(smd_ctx *ctx, long long job_id);
+/* Stop the context's serving worker after the queued jobs (call before
+ * smd_ctx_destroy when smd_submit was used). */
+SMD_API void smd_serve_shutdown(smd_ctx *ctx);
+
+/* ---------------------------------------------------------- diagnostics */
+
+/* Measured FMA throughput (TFLOP/s, 2 flops per FMA) of the device in the
+ * given precision; the roofline denominator of the RK kernels.  No
+ * counterpart in the reference (it has no device code). */
+SMD_API int smd_measure_fma_peak(int device, int precision, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

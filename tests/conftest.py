@@ -1,0 +1,44 @@
+import glob
+import json
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a B200 (sm_100) GPU and the built CUDA library")
+
+
+def load_golden(name):
+    from classical_mc_and_smd_for_2d_heisenberg_models_b200.settings import SMDSettings
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    d = {k: z[k] for k in z.files}
+    s = SMDSettings(**{k: v for k, v in json.loads(str(d["settings"])).items()})
+    return s, d
+
+
+def golden_names(prefix=""):
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, prefix + "*.npz")))
+
+
+@pytest.fixture(scope="session")
+def oracle_mod():
+    import oracle
+    oracle.build()
+    return oracle
+
+
+@pytest.fixture(scope="session")
+def ctx():
+    """A device context; on a GPU box a missing library or device is an error."""
+    from classical_mc_and_smd_for_2d_heisenberg_models_b200.smd import Context
+    c = Context(0)
+    yield c
+    c.close()

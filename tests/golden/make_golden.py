@@ -1,0 +1,106 @@
+"""Generate the golden fixtures of tests/golden/ from the reference itself.
+
+The reference ships no test vectors for its SMD path, so the fixtures are
+produced by running the reference's own code: oracle/_ref/smd_ref_run is
+Codes_Folder/subrouts.cpp compiled from its sources (see oracle/Makefile),
+driven through the same calls its main program makes.  Inputs are seeded
+synthetic samples in the reference's sample-file format.
+
+Every case stores: the settings, the reference's lattice tables (positions,
+grid map, neighbour tables, bond list), the input samples and impurity map,
+the reference's final spins after ntm - 1 RK steps, and the reference's sums
+over samples of |S(q,w)|^2 and of the autocorrelation.
+
+Run from the repository root (needs the reference sources at build time):
+    make -C oracle ref && python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import dataclasses
+import json
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import oracle as O  # noqa: E402
+from classical_mc_and_smd_for_2d_heisenberg_models_b200 import samples as smp  # noqa: E402
+from classical_mc_and_smd_for_2d_heisenberg_models_b200.settings import SMDSettings  # noqa: E402
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+# (name, settings overrides, ntm, samples, ordered state, tilt sigma, seed)
+CASES = [
+    # 200-step per-spin trajectories, the north-star parity window
+    ("traj_square_j1j2", dict(geom="square", L=8, J2=0.6, dtm=0.01), 201, 2, "stripe", 0.2, 11),
+    ("traj_triang_j1j2", dict(geom="triang", L=6, J2=0.12, dtm=0.02), 201, 2, "q120", 0.15, 12),
+    ("traj_square_xxz_h_vac", dict(geom="square", L=8, J2=0.55, JX=0.1, zlamb1=0.9, zlamb2=0.9,
+                                   h=0.3, imp_ratio=0.05, dtm=0.01), 201, 2, "stripe", 0.1, 13),
+    ("traj_kagome", dict(geom="kagome", L=6, J2=0.3, JX=0.1, dtm=0.01), 201, 1, "ferro", 0.6, 14),
+    ("traj_hexagn", dict(geom="hexagn", L=6, J2=0.2, JX=0.05, dtm=0.01), 201, 1, "ferro", 0.6, 15),
+    ("traj_lieb_delta", dict(geom="lieb", L=6, J2=0.4, J2_delta=0.15, JX=0.05, dtm=0.01), 201, 1,
+     "ferro", 0.6, 16),
+    # short spectra over the full grid with a window
+    ("spec_square", dict(geom="square", L=4, J2=0.6, dtm=0.02, window="hann1"), 16, 2, "stripe",
+     0.3, 21),
+    ("spec_triang", dict(geom="triang", L=6, J2=0.12, h=0.2, dtm=0.02, window="black"), 16, 2,
+     "q120", 0.3, 22),
+    ("spec_hexagn", dict(geom="hexagn", L=6, J2=0.2, dtm=0.02, window="gauss"), 16, 2, "ferro",
+     0.7, 23),
+    ("spec_kagome", dict(geom="kagome", L=6, J2=0.3, JX=0.1, dtm=0.02, window="flatw"), 16, 2,
+     "ferro", 0.7, 24),
+    ("spec_lieb_disorder", dict(geom="lieb", L=4, J2=0.4, imp_ratio=0.1, J1ic=0.5, J2ic=0.2,
+                                J1ii=0.3, dtm=0.02, window="ntall"), 16, 2, "ferro", 0.7, 25),
+]
+
+
+def run_case(name, over, ntm, n, kind, sigma, seed, workroot):
+    s = SMDSettings(ntm=ntm, NMeas=1000 * max(n, 2), crSkip=1000, **over)
+    s.validate(check_dwf=False)
+    wd = os.path.join(workroot, name)
+    s.write(wd)
+    pack = s.pack_size
+    total = n if not s.disorder else pack * ((n + pack - 1) // pack)
+    if not s.disorder and total not in (1,) and total % pack:
+        total = pack * ((total + pack - 1) // pack)
+    spins, imp = smp.make_samples(s, total, kind, sigma, seed)
+    path = os.path.join(wd, "samples.bin")
+    smp.write_sample_file(path, s, spins, imp)
+    info = O.run_reference(wd, path, 0, n, dump_final=True, dwf_guard=False)
+    lat = O.read_ref_lattice(wd)
+    spec, qss = O.read_ref_spec(wd, s.G * s.G, ntm)
+    final = O.read_ref_final(wd, n, s.N)
+    win = O.window(s.window, ntm) if s.window != "nowin" else np.ones(ntm)
+    out = dict(
+        settings=json.dumps(dataclasses.asdict(s)),
+        spins0=spins[:n], final=final, spec_sum=spec, qss_sum=qss,
+        rvec=lat["rvec"], grid_map=lat["grid_map"], nb1=lat["nbrs"][0], nb2=lat["nbrs"][1],
+        nbx=lat["nbrs"][2], bonds=lat["bonds"], nbonds=np.array(lat["nbonds"], np.int32),
+        window=win, n=np.int32(n),
+    )
+    if imp is not None:
+        out["imp"] = imp[0]
+    if name.startswith("traj_"):
+        # trajectories keep only the final spins; the spectrum is not needed
+        out.pop("spec_sum")
+        out.pop("qss_sum")
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+    return info
+
+
+def main():
+    if not O.reference_available():
+        raise SystemExit("oracle/_ref/smd_ref_run is missing: run `make -C oracle ref` first")
+    with tempfile.TemporaryDirectory() as tmp:
+        for c in CASES:
+            info = run_case(*c, tmp)
+            print(c[0], info)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,148 @@
+"""CUDA path against the oracle and the reference's own outputs (B200 only).
+
+Tolerances (FP64 plain form), as the path's contract states them:
+  * per spin, within 1e-10 of the reference over the first 200 steps;
+  * spectra and autocorrelation of short runs: max |diff| <= 1e-10 of max |ref|.
+The GPU correction step updates all sites from one set of fields (Jacobi)
+where the reference updates in site order; the difference is O(scale^2) per
+step, far below these bounds.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden_names, load_golden
+from classical_mc_and_smd_for_2d_heisenberg_models_b200 import _lib, smd
+from classical_mc_and_smd_for_2d_heisenberg_models_b200 import samples as smp
+from classical_mc_and_smd_for_2d_heisenberg_models_b200.settings import SMDSettings
+
+pytestmark = pytest.mark.gpu
+
+SPIN_TOL = 1e-10
+SPEC_TOL = 1e-10
+
+
+def _upload(ctx, s):
+    lat = smd.build_lattice(s.geom, s.L)
+    return lat, ctx.lattice(s, lat)
+
+
+@pytest.mark.parametrize("name", golden_names("traj_"))
+def test_fp64_200_steps_per_spin(ctx, name):
+    s, d = load_golden(name)
+    lat, lid = _upload(ctx, s)
+    n = int(d["n"])
+    imp = None if "imp" not in d else np.tile(d["imp"], (n, 1))
+    fin = ctx.evolve(lid, d["spins0"][:n], s.dtm, s.ntm - 1, imp=imp)
+    err = np.max(np.abs(fin - d["final"]))
+    assert err <= SPIN_TOL, err
+
+
+@pytest.mark.parametrize("name", golden_names("spec_"))
+def test_fp64_spectrum_equals_reference(ctx, name):
+    s, d = load_golden(name)
+    lat, lid = _upload(ctx, s)
+    qid = ctx.qset(lid, use_grid=True)
+    n = int(d["n"])
+    imp = None if "imp" not in d else np.tile(d["imp"], (n, 1))
+    r = ctx.run(lid, qid, d["spins0"][:n], s.dtm, s.ntm, win=d["window"], imp=imp)
+    ref = d["spec_sum"] / n
+    assert np.max(np.abs(r.spec - ref)) <= SPEC_TOL * np.max(np.abs(ref))
+    assert np.max(np.abs(r.qss - d["qss_sum"] / n)) <= SPEC_TOL
+    assert np.max(np.abs(r.final - d["final"])) <= SPIN_TOL
+
+
+def test_reference_entry_point(ctx):
+    """smd_dyn_spectrum_ref: the data of get_dynSpectrum with flat arrays."""
+    s, d = load_golden("spec_triang")
+    lat, lid = _upload(ctx, s)
+    qid = ctx.qset(lid, use_grid=True)
+    sf = d["spins0"][0].copy()
+    x, y, z, q = ctx.get_dyn_spectrum(lid, qid, s.dtm, s.ntm, d["window"], sf)
+    assert np.max(np.abs(sf - d["final"][0])) <= SPIN_TOL
+    assert x.shape == (s.G * s.G, s.ntm)
+    assert q[0] == 1.0
+
+
+@pytest.mark.parametrize("geom,L,J2,JX,stride,n_rec", [
+    ("square", 16, 0.6, 0.0, 4, 64),
+    ("triang", 12, 0.12, 0.0, 2, 48),
+    ("kagome", 6, 0.3, 0.1, 3, 40),
+    ("hexagn", 6, 0.2, 0.05, 2, 30),
+])
+def test_fp64_strided_grid_and_list_vs_oracle(ctx, oracle_mod, geom, L, J2, JX, stride, n_rec):
+    s = SMDSettings(geom=geom, L=L, J2=J2, JX=JX, dtm=0.01, ntm=n_rec, window="hann1",
+                    NMeas=4000)
+    lat, lid = _upload(ctx, s)
+    rng = np.random.default_rng(3)
+    ql = rng.uniform(-np.pi, np.pi, size=(7, 2))
+    qid = ctx.qset(lid, use_grid=True, qlist=ql)
+    kind = "q120" if geom == "triang" else ("stripe" if geom == "square" else "ferro")
+    spins, _ = smp.make_samples(s, 3, kind, 0.4, 9)
+    win = smd.window("hann1", n_rec)
+    r = ctx.run(lid, qid, spins, s.dtm, n_rec, stride=stride, win=win)
+    olat = oracle_mod.make_lattice(geom, L)
+    m = oracle_mod.Model(s, olat)
+    acc, accq = 0.0, 0.0
+    for k in range(3):
+        o = oracle_mod.dyn_spectrum(m, spins[k], s.dtm, n_rec, stride=stride, win=win,
+                                    qlist=ql, pos=lat.grid_positions(), list_scale=1.0 / lat.G)
+        acc = acc + o["spec"]
+        accq = accq + o["qss"]
+        assert np.max(np.abs(r.final[k] - o["final"])) <= SPIN_TOL
+    acc /= 3
+    accq /= 3
+    assert np.max(np.abs(r.spec - acc)) <= SPEC_TOL * np.max(np.abs(acc))
+    assert np.max(np.abs(r.qss - accq)) <= SPEC_TOL
+
+
+def test_list_points_on_the_grid_equal_grid_values(ctx):
+    s = SMDSettings(geom="kagome", L=6, J2=0.3, dtm=0.01, ntm=16)
+    lat, lid = _upload(ctx, s)
+    gq = lat.grid_qvectors()
+    pick = np.array([0, 5, 17, 40, 143])
+    qid = ctx.qset(lid, use_grid=True, qlist=gq[pick])
+    spins, _ = smp.make_samples(s, 2, "ferro", 0.5, 4)
+    r = ctx.run(lid, qid, spins, s.dtm, 16)
+    G2 = lat.G * lat.G
+    a = r.spec[:, pick, :]
+    b = r.spec[:, G2:, :]
+    assert np.max(np.abs(a - b)) <= 1e-11 * np.max(np.abs(a))
+
+
+def test_runs_are_deterministic(ctx):
+    s = SMDSettings(geom="square", L=16, J2=0.6, dtm=0.01, ntm=32)
+    lat, lid = _upload(ctx, s)
+    qid = ctx.qset(lid)
+    spins, _ = smp.make_samples(s, 4, "stripe", 0.2, 1)
+    a = ctx.run(lid, qid, spins, s.dtm, 32, stride=2)
+    b = ctx.run(lid, qid, spins, s.dtm, 32, stride=2)
+    assert np.array_equal(a.spec, b.spec) and np.array_equal(a.final, b.final)
+
+
+def test_fp32_form_energy_and_spectrum_error(ctx):
+    """Precision form: FP32 stages, FP64 correction every 16 steps."""
+    s = SMDSettings(geom="triang", L=48, J2=0.12, dtm=0.02, ntm=256, window="hann1")
+    lat, lid = _upload(ctx, s)
+    qid = ctx.qset(lid)
+    spins, _ = smp.make_samples(s, 8, "q120", 0.15, 2)
+    win = smd.window("hann1", 256)
+    r64 = ctx.run(lid, qid, spins, s.dtm, 256, stride=4, win=win)
+    r32 = ctx.run(lid, qid, spins, s.dtm, 256, stride=4, win=win, precision=_lib.SMD_FP32,
+                  fix_every=16)
+    rel = np.linalg.norm(r32.spec - r64.spec) / np.linalg.norm(r64.spec)
+    assert rel <= 1e-3, rel
+    assert r32.report["drift_final"] <= 1e-8, r32.report
+    assert r32.report["drift_max"] <= 1e-8, r32.report
+
+
+def test_invalid_jobs_fail_loudly(ctx):
+    s = SMDSettings(geom="square", L=8, J2=0.6, dtm=0.01, ntm=16)
+    lat, lid = _upload(ctx, s)
+    qid = ctx.qset(lid)
+    spins, _ = smp.make_samples(s, 1, "stripe", 0.2, 1)
+    with pytest.raises(_lib.SMDError):
+        ctx.run(lid, qid, spins, -0.01, 16)
+    with pytest.raises(_lib.SMDError):
+        ctx.run(lid, qid + 1000, spins, 0.01, 16)
+    with pytest.raises(_lib.SMDError):
+        ctx.run(lid, qid, spins, 0.01, 1)
