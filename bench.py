@@ -373,11 +373,20 @@ def main():
     ap.add_argument("--ref-ntm", type=int, default=1025)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--records", type=int, default=0,
+                    help="override the record count (small profiling cases only)")
+    ap.add_argument("--samples", type=int, default=0,
+                    help="override the samples per GPU (small profiling cases only)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     from classical_mc_and_smd_for_2d_heisenberg_models_b200 import workloads
+    import dataclasses
     w = workloads.WORKLOADS[args.workload]()
+    if args.records:
+        w = dataclasses.replace(w, n_rec=args.records)
+    if args.samples:
+        w = dataclasses.replace(w, n_samples=args.samples)
     if args.impl == "reference":
         line = run_reference_arm(args, w, rank, world)
     else:
