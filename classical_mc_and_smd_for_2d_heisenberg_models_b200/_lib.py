@@ -27,7 +27,7 @@ EXPORTS = [
     "smd_lattice_upload", "smd_lattice_free", "smd_qset_upload", "smd_qset_size",
     "smd_lattice_sites", "smd_run", "smd_run_device", "smd_dyn_spectrum_ref",
     "smd_evolve", "smd_submit", "smd_poll", "smd_wait", "smd_cancel",
-    "smd_serve_shutdown", "smd_measure_fma_peak",
+    "smd_serve_shutdown", "smd_evolve_fp64_noalloc", "smd_measure_fma_peak",
 ]
 
 
@@ -54,6 +54,14 @@ class JobDesc(C.Structure):
     _fields_ = [("lattice", C.c_int), ("qset", C.c_int), ("n_samples", C.c_int),
                 ("dt", C.c_double), ("n_rec", C.c_int), ("stride", C.c_int),
                 ("precision", C.c_int), ("fix_every", C.c_int), ("imp", C.c_void_p)]
+
+
+class NoAllocModel(C.Structure):
+    _fields_ = [("N", C.c_int), ("zn", C.c_int * 3), ("d_nbr", C.c_void_p),
+                ("J", C.c_double * 3), ("lambda_", C.c_double * 9), ("h", C.c_double)]
+
+
+NOALLOC_SCRATCH_BYTES = 16 << 20
 
 
 class Report(C.Structure):
@@ -104,6 +112,8 @@ def load():
     L.smd_cancel.argtypes = [vp, C.c_longlong]
     L.smd_serve_shutdown.argtypes = [vp]
     L.smd_serve_shutdown.restype = None
+    L.smd_evolve_fp64_noalloc.argtypes = [C.POINTER(NoAllocModel), C.c_int, C.c_double, C.c_int,
+                                          vp, vp, vp]
     L.smd_measure_fma_peak.argtypes = [C.c_int, C.c_int, dp]
     _lib = L
     return L

@@ -219,6 +219,46 @@ SMD_API int smd_cancel(smd_ctx *ctx, long long job_id);
  * smd_ctx_destroy when smd_submit was used). */
 SMD_API void smd_serve_shutdown(smd_ctx *ctx);
 
+/* ------------------------------------------------- allocation-free entry */
+
+/* Bytes of the static device array behind smd_evolve_fp64_noalloc. */
+#define SMD_NOALLOC_SCRATCH_BYTES (16u << 20)
+
+/* Model of smd_evolve_fp64_noalloc: a lattice without disorder or d-wave
+ * term, whose neighbour table the caller keeps in device memory. */
+typedef struct {
+    int N;                 /* sites */
+    int zn[3];             /* neighbours per shell; 0 switches a shell off */
+    const int *d_nbr;      /* DEVICE table [zn0 + zn1 + zn2][N]: row zoff(s) + k holds
+                              the k-th neighbour of shell s of every site (the
+                              transpose of smd_build_lattice's [N][zn] tables) */
+    double J[3];           /* J1, J2, JX */
+    double lambda[3][3];   /* lambdaVec1..3 */
+    double h;              /* field along z */
+} smd_noalloc_model;
+
+/* FP64 RK4 + energy-correction evolution (nsteps steps, correction every
+ * step) of n_samples samples that allocates no device memory: no
+ * cudaMalloc, cudaFree or allocating library call.  No counterpart in the
+ * reference.  It serves callers that own all device memory themselves (a
+ * framework's memory pool, or a real-time loop that may not allocate once
+ * running) and so cannot let this library call cudaMalloc.
+ *   d_spins_in, d_spins_out: DEVICE [n_samples][N][3] (may be the same buffer)
+ *   stream: cudaStream_t to enqueue on (NULL = default stream); the call
+ *           returns once the work is enqueued.
+ * Working memory comes from one static device array of
+ * SMD_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until
+ * exit; a call needs about n_samples * (96 N + 56) bytes of it and returns
+ * SMD_ENOMEM_ADMIT when that exceeds the array.  The first call on a device
+ * looks up the array's address (cudaGetSymbolAddress) with that device
+ * current: make it before any stream capture.  All calls share the array and
+ * it keeps the last call's contents, so calls that overlap on the GPU race:
+ * serialise them.  The tables must list every neighbour relation once in
+ * each direction (true for smd_build_lattice tables with L >= 4). */
+SMD_API int smd_evolve_fp64_noalloc(const smd_noalloc_model *m, int n_samples, double dt,
+                                    int nsteps, const double *d_spins_in, double *d_spins_out,
+                                    void *stream);
+
 /* ---------------------------------------------------------- diagnostics */
 
 /* Measured FMA throughput (TFLOP/s, 2 flops per FMA) of the device in the
