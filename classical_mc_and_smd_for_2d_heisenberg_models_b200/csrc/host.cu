@@ -16,6 +16,7 @@
 // windows, transforms and squares every series and adds the sum over the
 // wave's samples into the job's accumulator.
 #include "../../include/smd_b200.h"
+#include "rk_cluster.cuh"
 #include "smd_launch.h"
 
 #include <cuda_runtime.h>
@@ -24,6 +25,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -61,12 +63,21 @@ struct DevBuf {
     T *as() const { return static_cast<T *>(p); }
 };
 
+// Partition of one lattice over a cluster of CS CTAs (see rk_cluster.cuh).
+struct ClusterTab {
+    ClusterParams P{};
+    DevBuf own_base, own_cnt, halo_cnt, halo_gid, idx, push;
+};
+
 struct Lattice {
     int N = 0, G = 0, zn[3] = {0, 0, 0}, zoff[3] = {0, 0, 0}, ztot = 0;
     bool lieb_delta = false;
+    bool vac_only = true;           // impurities (if any) have zero couplings
     LatticeDev dev{};
     DevBuf nbr, grid_map, bonds;
     std::vector<double> pos;
+    std::vector<int> nbr_h[3];      // host copies of the active shells' tables
+    std::map<int, std::unique_ptr<ClusterTab>> ctabs;   // keyed by CTAs per sample
 };
 
 struct QSet {
@@ -364,6 +375,13 @@ extern "C" int smd_lattice_upload(smd_ctx *ctx, const smd_lattice_desc *d, int *
     v.nbonds = nb;
     v.bonds = L->bonds.as<int4>();
     L->lieb_delta = v.lieb_delta_on;
+    for (int s = 0; s < 3; s++) {
+        for (int a = 0; a < 2; a++)
+            for (int b = 0; b < 2; b++)
+                if ((a || b) && d->J[s][a][b] != 0.0) L->vac_only = false;
+        if (v.shell_on[s])
+            L->nbr_h[s].assign(d->nbr[s], d->nbr[s] + (size_t)N * d->zn[s]);
+    }
     const int id = ctx->next_id++;
     ctx->lattices[id] = std::move(L);
     *lattice_id = id;
@@ -443,7 +461,170 @@ struct JobGeom {
     Plan *tp;
     int N, Q, n_rec, prec, R, W, waves;
     size_t elem, celem;
+    ClusterTab *ctab = nullptr;   // cluster kernel partition (null: single-CTA kernel)
+    int spt = 0, threads = 0;
 };
+
+// Partition of lattice L over CS CTAs: contiguous site ranges, halo lists,
+// packed local neighbour slots and halo push lists.  Null when the lattice
+// does not fit the cluster kernel's limits.
+ClusterTab *cluster_tables(Lattice &L, int CS)
+{
+    auto it = L.ctabs.find(CS);
+    if (it != L.ctabs.end()) return it->second.get();
+    const int N = L.N;
+    if (CS < 1 || CS > kMaxClusterCTAs || N < CS) return nullptr;
+    const int zact = L.zn[0] + L.zn[1] + L.zn[2];
+    const int ZT = zact <= 4 ? 4 : zact <= 8 ? 8 : zact <= 12 ? 12 : zact <= 18 ? 18 : -1;
+    if (ZT < 0) return nullptr;
+    std::vector<int> base(CS + 1), owner(N);
+    for (int r = 0; r <= CS; r++) base[r] = (int)((long long)N * r / CS);
+    for (int r = 0; r < CS; r++)
+        for (int g = base[r]; g < base[r + 1]; g++) owner[g] = r;
+    // neighbours of site g over the active shells, in edge-slot order
+    auto edge = [&](int g, int e) -> int {
+        for (int s = 0; s < 3; s++) {
+            if (e < L.zn[s]) return L.nbr_h[s][(size_t)g * L.zn[s] + e];
+            e -= L.zn[s];
+        }
+        return -1;
+    };
+    std::vector<std::vector<int>> halo(CS);
+    int n_own_max = 0, n_loc_max = 0;
+    for (int r = 0; r < CS; r++) {
+        std::set<int> hs;
+        for (int g = base[r]; g < base[r + 1]; g++)
+            for (int e = 0; e < zact; e++) {
+                const int j = edge(g, e);
+                if (j >= 0 && owner[j] != r) hs.insert(j);
+            }
+        halo[r].assign(hs.begin(), hs.end());
+        const int own = base[r + 1] - base[r];
+        n_own_max = std::max(n_own_max, own);
+        n_loc_max = std::max(n_loc_max, own + (int)halo[r].size());
+    }
+    if (n_loc_max + 1 > 65536) return nullptr;
+    const int pad = n_loc_max;
+    std::vector<uint32_t> idx((size_t)CS * (ZT / 2) * n_own_max, (uint32_t)pad | ((uint32_t)pad << 16));
+    std::vector<int> hgid((size_t)CS * n_loc_max, 0);
+    std::vector<std::vector<std::vector<int>>> pushes(CS);
+    for (int r = 0; r < CS; r++) pushes[r].resize(base[r + 1] - base[r]);
+    for (int r = 0; r < CS; r++) {
+        const int own = base[r + 1] - base[r];
+        std::map<int, int> hslot;
+        for (size_t q = 0; q < halo[r].size(); q++) {
+            const int j = halo[r][q];
+            hslot[j] = own + (int)q;
+            hgid[(size_t)r * n_loc_max + q] = j;
+            const int o = owner[j];
+            pushes[o][j - base[o]].push_back((r << 16) | (own + (int)q));
+        }
+        for (int li = 0; li < own; li++) {
+            const int g = base[r] + li;
+            for (int e = 0; e < ZT; e++) {
+                int sl = pad;
+                const int j = e < zact ? edge(g, e) : -1;
+                if (j >= 0) sl = (owner[j] == r) ? j - base[r] : hslot[j];
+                uint32_t &w = idx[((size_t)r * (ZT / 2) + e / 2) * n_own_max + li];
+                if (e % 2 == 0) w = (w & 0xffff0000u) | (uint32_t)sl;
+                else w = (w & 0x0000ffffu) | ((uint32_t)sl << 16);
+            }
+        }
+    }
+    int pmax = 0;
+    for (int r = 0; r < CS; r++)
+        for (auto &v : pushes[r]) pmax = std::max(pmax, (int)v.size());
+    std::vector<int> push((size_t)CS * std::max(pmax, 1) * n_own_max, -1);
+    for (int r = 0; r < CS; r++)
+        for (size_t li = 0; li < pushes[r].size(); li++)
+            for (size_t p = 0; p < pushes[r][li].size(); p++)
+                push[((size_t)r * pmax + p) * n_own_max + li] = pushes[r][li][p];
+    std::vector<int> cnt(CS), hc(CS);
+    for (int r = 0; r < CS; r++) {
+        cnt[r] = base[r + 1] - base[r];
+        hc[r] = (int)halo[r].size();
+    }
+
+    auto T = std::make_unique<ClusterTab>();
+    ClusterParams &P = T->P;
+    P.N = N;
+    P.CS = CS;
+    P.n_own_max = n_own_max;
+    P.n_loc_max = n_loc_max;
+    P.pmax = pmax;
+    P.ZT = ZT;
+    P.energy_from_field = L.dev.energy_from_field;
+    P.h = L.dev.h;
+    P.hf = (float)L.dev.h;
+    for (int e = 0; e < kMaxEdgeSlots; e++)
+        for (int c = 0; c < 3; c++) {
+            P.coef64[e][c] = 0.0;
+            P.coef32[e][c] = 0.0f;
+        }
+    for (int e = 0; e < zact; e++) {
+        int s = 0, k = e;
+        while (k >= L.zn[s]) k -= L.zn[s++];
+        for (int c = 0; c < 3; c++) {
+            P.coef64[e][c] = L.dev.coef[s][c];
+            P.coef32[e][c] = (float)L.dev.coef[s][c];
+        }
+    }
+    auto up = [](DevBuf &b, const void *src, size_t bytes) {
+        if (b.ensure(std::max<size_t>(bytes, 4)) != cudaSuccess) return false;
+        return cudaMemcpy(b.p, src, bytes, cudaMemcpyHostToDevice) == cudaSuccess;
+    };
+    if (!up(T->own_base, base.data(), CS * sizeof(int)) || !up(T->own_cnt, cnt.data(), CS * sizeof(int)) ||
+        !up(T->halo_cnt, hc.data(), CS * sizeof(int)) ||
+        !up(T->halo_gid, hgid.data(), hgid.size() * sizeof(int)) ||
+        !up(T->idx, idx.data(), idx.size() * sizeof(uint32_t)) ||
+        !up(T->push, push.data(), push.size() * sizeof(int)))
+        return nullptr;
+    P.own_base = T->own_base.as<int>();
+    P.own_cnt = T->own_cnt.as<int>();
+    P.halo_cnt = T->halo_cnt.as<int>();
+    P.halo_gid = T->halo_gid.as<int>();
+    P.idx = T->idx.as<uint32_t>();
+    P.push = T->push.as<int>();
+    ClusterTab *raw = T.get();
+    L.ctabs[CS] = std::move(T);
+    return raw;
+}
+
+// Cluster size and thread shape for a job.  Lattices the cluster kernel does
+// not cover (bond-list energies, the Lieb d-wave term, impurities with
+// non-zero couplings) keep the single-CTA kernel.  Otherwise the smallest
+// cluster that puts at least ~85% of the SMs to work is taken, within the
+// shared-memory and register limits; SMD_CLUSTER_CTAS forces a size.
+void choose_cluster(smd_ctx *ctx, JobGeom &g, int n_samples)
+{
+    Lattice &L = *g.L;
+    g.ctab = nullptr;
+    if (!L.dev.energy_from_field || L.lieb_delta || !L.vac_only) return;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    int forced = 0;
+    if (const char *e = std::getenv("SMD_CLUSTER_CTAS")) forced = std::atoi(e);
+    const int sizes[] = {1, 2, 4, 8, 16};
+    for (int CS : sizes) {
+        if (forced && CS != forced) continue;
+        if (!forced && CS > 1 && L.N / CS < 96) break;
+        ClusterTab *t = cluster_tables(L, CS);
+        if (!t) continue;
+        int spt = 0;
+        for (int s : {1, 2, 4})
+            if (s * rk_cluster_maxt(g.prec, s) >= t->P.n_own_max) {
+                spt = s;
+                break;
+            }
+        if (!spt) continue;
+        if (rk_cluster_smem(t->P, g.prec) > 227 * 1024) continue;
+        g.ctab = t;
+        g.spt = spt;
+        g.threads = std::max(32, (t->P.n_own_max + spt - 1) / spt + 31) / 32 * 32;
+        g.threads = std::min(g.threads, rk_cluster_maxt(g.prec, spt));
+        if (forced || (long long)n_samples * CS >= (long long)(0.85 * sms)) return;
+    }
+}
 
 int prepare(smd_ctx *ctx, const smd_job_desc *job, JobGeom &g)
 {
@@ -467,7 +648,8 @@ int prepare(smd_ctx *ctx, const smd_job_desc *job, JobGeom &g)
     g.Q = g.Qs->Q;
     g.n_rec = job->n_rec;
     g.prec = job->precision;
-    if (g.N > rk_max_sites(g.prec))
+    choose_cluster(ctx, g, job->n_samples);
+    if (!g.ctab && g.N > rk_max_sites(g.prec))
         return fail(ctx, SMD_EINVAL, "job: N exceeds the single-CTA capacity of this form");
     if (g.Qs->use_grid && g.prec == SMD_FP64 && !g.Qs->fp64_ok)
         return fail(ctx, SMD_EINVAL, "job: grid too large for the FP64 shared-memory transform");
@@ -581,7 +763,10 @@ int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const do
             J.stats = ctx->stats.as<double>();
             J.status = ctx->status.as<int>();
             CK(cudaEventRecord(ev(2 + 2 * c), ctx->s_rk), "event");
-            CK(launch_rk(L.dev, J, g.prec, gen, ctx->s_rk), "rk kernel");
+            if (g.ctab)
+                CK(launch_rk_cluster(g.ctab->P, J, g.prec, g.spt, g.threads, ctx->s_rk), "rk cluster kernel");
+            else
+                CK(launch_rk(L.dev, J, g.prec, gen, ctx->s_rk), "rk kernel");
             CK(cudaEventRecord(ev(3 + 2 * c), ctx->s_rk), "event");
             ctx->launches++;
             rk_launches++;

@@ -1,0 +1,51 @@
+// rk_cluster.cuh -- RK4 + energy-correction kernel for one sample spread over
+// a thread-block cluster (declarations shared by host and device code).
+//
+// A sample's N sites are cut into CS contiguous index ranges, one per CTA of
+// a cluster.  Each CTA keeps in shared memory the stage values of its own
+// sites and of the halo sites (other CTAs' sites that its sites neighbour).
+// After computing a stage value a thread stores it locally and pushes it
+// into the halo slots of the CTAs that hold a copy (distributed shared
+// memory stores); one cluster barrier per stage publishes everything.
+//
+// Site records are 4-wide vectors (x, y, z, 0), so a neighbour costs one
+// vector load; neighbours are local slot numbers packed two per 32-bit word;
+// every edge slot e has one coefficient vector J_shell(e) * lambda_shell(e)
+// passed as a kernel parameter, which the unrolled edge loop reads as a
+// constant operand.  Vacancies (impurities with zero couplings) are handled
+// by storing mask * S in the gathered buffers, mask = 1 - impurity flag.
+#pragma once
+
+#include "smd_device.cuh"
+
+namespace smd {
+
+constexpr int kMaxEdgeSlots = 18;
+constexpr int kMaxClusterCTAs = 16;
+
+struct ClusterParams {
+    int N;
+    int CS;                // CTAs per sample
+    int n_own_max;         // largest own range
+    int n_loc_max;         // largest own + halo count
+    int pmax;              // push entries per own site
+    int ZT;                // edge slots (padded to the kernel's template value)
+    int energy_from_field; // must be 1 (host routes other lattices elsewhere)
+    double h;
+    float hf;
+    double coef64[kMaxEdgeSlots][3];
+    float coef32[kMaxEdgeSlots][3];
+    const int *own_base;   // [CS]
+    const int *own_cnt;    // [CS]
+    const int *halo_cnt;   // [CS]
+    const int *halo_gid;   // [CS][n_loc_max]
+    const uint32_t *idx;   // [CS][ZT/2][n_own_max] packed local slots
+    const int *push;       // [CS][pmax][n_own_max] (rank << 16 | slot) or -1
+};
+
+size_t rk_cluster_smem(const ClusterParams &P, int precision);
+int rk_cluster_maxt(int precision, int spt);
+cudaError_t launch_rk_cluster(const ClusterParams &P, const RKJob &J, int precision, int spt,
+                              int threads, cudaStream_t st);
+
+}  // namespace smd

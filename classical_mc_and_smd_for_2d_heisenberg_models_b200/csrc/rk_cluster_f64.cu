@@ -1,0 +1,32 @@
+// rk_cluster_f64.cu -- FP64 plain-form instantiations of the cluster RK
+// kernel, the shared-memory size rule and the precision dispatch.
+#include "rk_cluster_impl.cuh"
+
+namespace smd {
+
+cudaError_t launch_rk_cluster_f32(const ClusterParams &P, const RKJob &J, int spt, int threads,
+                                  size_t smem, cudaStream_t st);
+
+size_t rk_cluster_smem(const ClusterParams &P, int precision)
+{
+    const size_t v4 = precision == 0 ? 32 : 16;
+    const size_t Np = (size_t)P.n_loc_max + 1;
+    size_t b = 2 * Np * v4 + (size_t)(P.ZT / 2) * P.n_own_max * 4 + (size_t)P.pmax * P.n_own_max * 4;
+    b = (b + 15) & ~size_t(15);
+    return b + 2 * kMaxClusterCTAs * 4 * sizeof(double) + 32 * 4 * sizeof(double);
+}
+
+int rk_cluster_maxt(int precision, int spt)
+{
+    return precision == 0 ? cl_maxt<double>(spt) : cl_maxt<float>(spt);
+}
+
+cudaError_t launch_rk_cluster(const ClusterParams &P, const RKJob &J, int precision, int spt,
+                              int threads, cudaStream_t st)
+{
+    const size_t smem = rk_cluster_smem(P, precision);
+    if (precision == 0) return launch_cluster_prec<double>(P, J, spt, threads, smem, st);
+    return launch_rk_cluster_f32(P, J, spt, threads, smem, st);
+}
+
+}  // namespace smd

@@ -1,0 +1,568 @@
+// rk_cluster_impl.cuh -- the cluster RK kernel template (see rk_cluster.cuh).
+//
+// Per RK step, with A and B the two stage buffers (own + halo + one zero
+// pad slot) and S the FP64 master spins in registers
+// (Codes_Folder/subrouts.cpp:11734-11902):
+//
+//   stage 1  read A    write B = S + K1/2     (local store + halo pushes)  sync
+//   stage 2  read B    write A = S + K2/2                                  sync
+//   stage 3  read A    write B = S + K3                                    sync
+//   stage 4  read B    S = norm(S + (K1 + 2K2 + 2K3 + K4)/6)
+//   no fix:  write A = S                                                   sync
+//   fix:     FP64 field sweep, cluster reduction of sigma and E, S = norm(S +
+//            scale S x (h x S)) for every site from one set of fields, write A
+//
+// "sync" is one cluster barrier (release/acquire), which also orders the
+// distributed-shared-memory pushes.  The FP64 form (T = double) corrects
+// every step against the energy at the step's start, as the reference does;
+// the FP32 form (T = float) reuses the two FP32 buffers as one FP64 buffer
+// for its correction sweep every fix_every steps, against the initial
+// energy.  The reference corrects sites in order, each seeing its corrected
+// lower-index neighbours; the one-field (Jacobi) update here differs by
+// O(scale^2) per step, which is below 1e-20 for energy-conserving models
+// (lattices with the Lieb d-wave term are routed to the single-CTA kernel,
+// which reproduces the in-place order).
+#pragma once
+
+#include <cooperative_groups.h>
+
+#include "rk_cluster.cuh"
+
+namespace smd {
+
+namespace cg = cooperative_groups;
+
+template <typename T>
+struct alignas(4 * sizeof(T)) Vec4 {
+    T x, y, z, w;
+};
+
+__device__ __forceinline__ double cl_coef(const ClusterParams &P, int e, int c, double)
+{
+    return P.coef64[e][c];
+}
+__device__ __forceinline__ float cl_coef(const ClusterParams &P, int e, int c, float)
+{
+    return P.coef32[e][c];
+}
+
+// Register budget per own site: FP32 form 16 registers (FP64 spin, FP32
+// copy, stage input, accumulator, mask), FP64 form 19.
+template <typename T>
+__host__ __device__ constexpr int cl_maxt(int spt)
+{
+    return sizeof(T) == 4 ? (spt <= 1 ? 1024 : spt <= 2 ? 768 : 512)
+                          : (spt <= 1 ? 1024 : spt <= 2 ? 768 : 512);
+}
+
+template <typename T, int SPT, int ZT>
+__global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
+    rk_cluster_kernel(const ClusterParams P, const RKJob J)
+{
+    static_assert(ZT % 2 == 0 && ZT <= kMaxEdgeSlots, "edge slots come in packed pairs");
+    extern __shared__ __align__(32) unsigned char smem_raw[];
+    cg::cluster_group cl = cg::this_cluster();
+    const int CS = P.CS;
+    const int rank = (int)cl.block_rank();
+    const int smp = blockIdx.x / CS;
+    const int NT = blockDim.x, tid = threadIdx.x;
+    const int N = P.N;
+    const int base = P.own_base[rank], n_own = P.own_cnt[rank], n_halo = P.halo_cnt[rank];
+    const int nom = P.n_own_max;
+    const int Np = P.n_loc_max + 1;
+    const int pad = P.n_loc_max;
+    const T zero = T(0);
+
+    Vec4<T> *A = reinterpret_cast<Vec4<T> *>(smem_raw);
+    Vec4<T> *B = A + Np;
+    uint32_t *idx = reinterpret_cast<uint32_t *>(B + Np);
+    int *push = reinterpret_cast<int *>(idx + (ZT / 2) * nom);
+    size_t off = (size_t)(reinterpret_cast<unsigned char *>(push + P.pmax * nom) - smem_raw);
+    off = (off + 15) & ~size_t(15);
+    double *red = reinterpret_cast<double *>(smem_raw + off);   // [2][16][4]
+    double *wpart = red + 2 * kMaxClusterCTAs * 4;                // [32][4]
+    double *D = reinterpret_cast<double *>(smem_raw);             // [3][Np], FP32 form only
+
+    // ---- tables
+    {
+        const uint32_t *gi = P.idx + (size_t)rank * (ZT / 2) * nom;
+        for (int e = tid; e < (ZT / 2) * nom; e += NT) idx[e] = gi[e];
+        const int *gp = P.push + (size_t)rank * P.pmax * nom;
+        for (int e = tid; e < P.pmax * nom; e += NT) push[e] = gp[e];
+    }
+    const int *halo = P.halo_gid + (size_t)rank * P.n_loc_max;
+    const double *st = J.state + (size_t)smp * 3 * N;
+    const uint8_t *imp = J.imp ? J.imp + (size_t)smp * N : nullptr;
+
+    double S[SPT][3];
+    T mk[SPT];
+#pragma unroll
+    for (int k = 0; k < SPT; k++) {
+        const int li = tid + k * NT;
+        if (li < n_own) {
+            const int g = base + li;
+#pragma unroll
+            for (int c = 0; c < 3; c++) S[k][c] = st[c * N + g];
+            mk[k] = (imp && imp[g]) ? zero : T(1);
+        } else {
+#pragma unroll
+            for (int c = 0; c < 3; c++) S[k][c] = 0.0;
+            mk[k] = zero;
+        }
+    }
+    int slot = 0;
+    const double hz = P.h;
+
+    // ---- helpers
+    auto cl_sync = [&]() { cl.sync(); };
+
+    // Sum of NV doubles over every thread of every CTA of the cluster; all
+    // threads receive the totals, summed in a fixed order.
+    auto cluster_sum = [&](double *v, int NV) {
+        const int lane = tid & 31, warp = tid >> 5, nw = (NT + 31) >> 5;
+        for (int q = 0; q < NV; q++) v[q] = warp_sum(v[q]);
+        if (lane == 0)
+            for (int q = 0; q < NV; q++) wpart[warp * 4 + q] = v[q];
+        __syncthreads();
+        if (warp == 0) {
+            for (int q = 0; q < NV; q++) {
+                double x = (lane < nw) ? wpart[lane * 4 + q] : 0.0;
+                x = warp_sum(x);
+                if (lane == 0) {
+                    for (int r = 0; r < CS; r++) {
+                        double *rr = cl.map_shared_rank(red, r);
+                        rr[slot * kMaxClusterCTAs * 4 + rank * 4 + q] = x;
+                    }
+                }
+            }
+        }
+        cl.sync();
+        for (int q = 0; q < NV; q++) {
+            double s = 0.0;
+            for (int r = 0; r < CS; r++) s += red[slot * kMaxClusterCTAs * 4 + r * 4 + q];
+            v[q] = s;
+        }
+        slot ^= 1;
+    };
+
+    // local store of an own site's value plus the pushes into halo copies
+    auto put = [&](Vec4<T> *buf, int li, const Vec4<T> &v) {
+        buf[li] = v;
+        for (int p = 0; p < P.pmax; p++) {
+            const int code = push[p * nom + li];
+            if (code >= 0) {
+                Vec4<T> *rb = cl.map_shared_rank(buf, code >> 16);
+                rb[code & 0xffff] = v;
+            }
+        }
+    };
+    auto putD = [&](int li, const double v[3]) {
+        for (int c = 0; c < 3; c++) D[c * Np + li] = v[c];
+        for (int p = 0; p < P.pmax; p++) {
+            const int code = push[p * nom + li];
+            if (code >= 0) {
+                double *rd = cl.map_shared_rank(D, code >> 16);
+                const int s2 = code & 0xffff;
+                for (int c = 0; c < 3; c++) rd[c * Np + s2] = v[c];
+            }
+        }
+    };
+
+    // field of own site li from buffer src (mask_i applied, -h z added)
+    auto field = [&](const Vec4<T> *src, int li, T m, T h[3]) {
+        T s0 = zero, s1 = zero, s2 = zero;
+#pragma unroll
+        for (int e = 0; e < ZT; e += 2) {
+            const uint32_t w = idx[(e >> 1) * nom + li];
+            const Vec4<T> a = src[w & 0xffffu];
+            const Vec4<T> b = src[w >> 16];
+            s0 = fma(cl_coef(P, e, 0, zero), a.x, s0);
+            s1 = fma(cl_coef(P, e, 1, zero), a.y, s1);
+            s2 = fma(cl_coef(P, e, 2, zero), a.z, s2);
+            s0 = fma(cl_coef(P, e + 1, 0, zero), b.x, s0);
+            s1 = fma(cl_coef(P, e + 1, 1, zero), b.y, s1);
+            s2 = fma(cl_coef(P, e + 1, 2, zero), b.z, s2);
+        }
+        h[0] = m * s0;
+        h[1] = m * s1;
+        h[2] = m * s2 - T(hz);
+    };
+    auto field64 = [&](int li, double m, double h[3]) {
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+#pragma unroll
+        for (int e = 0; e < ZT; e += 2) {
+            const uint32_t w = idx[(e >> 1) * nom + li];
+            const int a = w & 0xffffu, b = w >> 16;
+            s0 = fma(P.coef64[e][0], D[a], s0);
+            s1 = fma(P.coef64[e][1], D[Np + a], s1);
+            s2 = fma(P.coef64[e][2], D[2 * Np + a], s2);
+            s0 = fma(P.coef64[e + 1][0], D[b], s0);
+            s1 = fma(P.coef64[e + 1][1], D[Np + b], s1);
+            s2 = fma(P.coef64[e + 1][2], D[2 * Np + b], s2);
+        }
+        h[0] = m * s0;
+        h[1] = m * s1;
+        h[2] = m * s2 - hz;
+    };
+    // own + halo values of the state from global memory (masked)
+    auto fill = [&](Vec4<T> *buf) {
+        for (int e = tid; e < n_own + n_halo; e += NT) {
+            const int g = e < n_own ? base + e : halo[e - n_own];
+            const T m = (imp && imp[g]) ? zero : T(1);
+            buf[e] = {m * T(st[g]), m * T(st[N + g]), m * T(st[2 * N + g]), zero};
+        }
+        if (tid == 0) {
+            A[pad] = {zero, zero, zero, zero};
+            B[pad] = {zero, zero, zero, zero};
+        }
+    };
+    auto fillD = [&]() {
+        for (int e = tid; e < n_own + n_halo; e += NT) {
+            const int g = e < n_own ? base + e : halo[e - n_own];
+            const double m = (imp && imp[g]) ? 0.0 : 1.0;
+            for (int c = 0; c < 3; c++) D[c * Np + e] = m * st[c * N + g];
+        }
+        if (tid == 0)
+            for (int c = 0; c < 3; c++) D[c * Np + pad] = 0.0;
+    };
+    auto normalise = [&](double v[3]) {
+        const double n2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+        if (sizeof(T) == 8) {
+            const double n = sqrt(n2);       // FP64 form: the reference's v / |v|
+            v[0] = v[0] / n;
+            v[1] = v[1] / n;
+            v[2] = v[2] / n;
+        } else {
+            const double r = rsqrt(n2);
+            v[0] *= r;
+            v[1] *= r;
+            v[2] *= r;
+        }
+    };
+    // FP64 energy of the state S (A holds it in the FP64 form; the FP32 form
+    // fills D from the owners first).  Call after a cluster barrier.
+    auto energy = [&]() -> double {
+        double e = 0.0;
+#pragma unroll
+        for (int k = 0; k < SPT; k++) {
+            const int li = tid + k * NT;
+            if (li < n_own) {
+                double h[3];
+                if (sizeof(T) == 8) {
+                    T ht[3];
+                    field(A, li, mk[k], ht);
+                    h[0] = ht[0]; h[1] = ht[1]; h[2] = ht[2];
+                } else {
+                    field64(li, (double)mk[k], h);
+                }
+                e += S[k][0] * h[0] + S[k][1] * h[1] + S[k][2] * h[2] - hz * S[k][2];
+            }
+        }
+        double v[1] = {e};
+        cluster_sum(v, 1);
+        return 0.5 * v[0];
+    };
+    auto publishD = [&]() {
+#pragma unroll
+        for (int k = 0; k < SPT; k++) {
+            const int li = tid + k * NT;
+            if (li < n_own) {
+                const double m = (double)mk[k];
+                const double v[3] = {m * S[k][0], m * S[k][1], m * S[k][2]};
+                putD(li, v);
+            }
+        }
+        if (tid == 0)
+            for (int c = 0; c < 3; c++) D[c * Np + pad] = 0.0;
+    };
+    auto publishA = [&]() {
+#pragma unroll
+        for (int k = 0; k < SPT; k++) {
+            const int li = tid + k * NT;
+            if (li < n_own) {
+                const T m = mk[k];
+                put(A, li, {m * T(S[k][0]), m * T(S[k][1]), m * T(S[k][2]), zero});
+            }
+        }
+        if (tid == 0) {
+            A[pad] = {zero, zero, zero, zero};
+            B[pad] = {zero, zero, zero, zero};
+        }
+    };
+    using TS = T;
+    TS *snap = reinterpret_cast<TS *>(J.snap);
+    const double *s0 = J.s0 + (size_t)smp * 3 * N;
+    auto record = [&](int r) {
+        const size_t sb = ((size_t)smp * J.snap_R + (r - J.rec_begin)) * 3 * N;
+        double p = 0.0;
+#pragma unroll
+        for (int k = 0; k < SPT; k++) {
+            const int li = tid + k * NT;
+            if (li < n_own) {
+                const int g = base + li;
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    snap[sb + (size_t)c * N + g] = (TS)S[k][c];
+                    p += s0[c * N + g] * S[k][c];
+                }
+            }
+        }
+        double v[1] = {p};
+        cluster_sum(v, 1);
+        if (rank == 0 && tid == 0) J.qss[(size_t)smp * J.n_rec + r] = (r == 0) ? 1.0 : (1.0 / N) * v[0];
+    };
+
+    cl_sync();   // every CTA of the cluster is running before any remote access
+
+    double E0, drift = 0.0;
+    if (J.rec_begin == 0) {
+        if (sizeof(T) == 8) {
+            fill(A);
+        } else {
+            fillD();
+        }
+        __syncthreads();
+        E0 = energy();
+        if (rank == 0 && tid == 0) J.e0[smp] = E0;
+        record(0);
+    } else {
+        E0 = J.e0[smp];
+        if (rank == 0 && tid == 0) drift = J.stats[smp * 4 + 0];
+    }
+    fill(A);
+    __syncthreads();
+    cl_sync();
+
+    const T dt = T(J.dt);
+    const T f1 = T(1.0 / 6.0), f2 = T(2.0 / 6.0);
+    const bool per_step = J.fix_every <= 1;
+    const int F = J.fix_every < 1 ? 1 : J.fix_every;
+    T Pin[SPT][3], acc[SPT][3];
+    for (int r = (J.rec_begin > 0 ? J.rec_begin : 1); r < J.rec_end; r++) {
+        for (int ss = 0; ss < J.stride; ss++) {
+            const int n = (r - 1) * J.stride + ss + 1;
+            const bool fix = per_step || (n % F == 0);
+            double eref = 0.0;
+            // ---- stage 1: A -> B
+#pragma unroll
+            for (int k = 0; k < SPT; k++) {
+                const int li = tid + k * NT;
+                if (li < n_own) {
+                    T h[3], Sp[3], Pv[3];
+                    field(A, li, mk[k], h);
+                    Sp[0] = T(S[k][0]);
+                    Sp[1] = T(S[k][1]);
+                    Sp[2] = T(S[k][2]);
+                    if (sizeof(T) == 8 && per_step)
+                        eref += S[k][0] * h[0] + S[k][1] * h[1] + S[k][2] * h[2] - hz * S[k][2];
+                    Pv[0] = h[1] * Sp[2] - h[2] * Sp[1];
+                    Pv[1] = h[2] * Sp[0] - h[0] * Sp[2];
+                    Pv[2] = h[0] * Sp[1] - h[1] * Sp[0];
+#pragma unroll
+                    for (int c = 0; c < 3; c++) {
+                        const T K = dt * Pv[c];
+                        acc[k][c] = f1 * K;
+                        Pin[k][c] = Sp[c] + T(0.5) * K;
+                    }
+                    const T m = mk[k];
+                    put(B, li, {m * Pin[k][0], m * Pin[k][1], m * Pin[k][2], zero});
+                }
+            }
+            cl_sync();
+            // ---- stages 2 and 3
+#pragma unroll
+            for (int stg = 0; stg < 2; stg++) {
+                const Vec4<T> *src = stg ? A : B;
+                Vec4<T> *dst = stg ? B : A;
+                const T cst = stg ? T(1) : T(0.5);
+#pragma unroll
+                for (int k = 0; k < SPT; k++) {
+                    const int li = tid + k * NT;
+                    if (li < n_own) {
+                        T h[3], Pv[3];
+                        field(src, li, mk[k], h);
+                        const T *Sp = Pin[k];
+                        Pv[0] = h[1] * Sp[2] - h[2] * Sp[1];
+                        Pv[1] = h[2] * Sp[0] - h[0] * Sp[2];
+                        Pv[2] = h[0] * Sp[1] - h[1] * Sp[0];
+                        T nx[3];
+#pragma unroll
+                        for (int c = 0; c < 3; c++) {
+                            const T K = dt * Pv[c];
+                            acc[k][c] += f2 * K;
+                            nx[c] = T(S[k][c]) + cst * K;
+                        }
+#pragma unroll
+                        for (int c = 0; c < 3; c++) Pin[k][c] = nx[c];
+                        const T m = mk[k];
+                        put(dst, li, {m * nx[0], m * nx[1], m * nx[2], zero});
+                    }
+                }
+                cl_sync();
+            }
+            // ---- stage 4 and the FP64 combination
+#pragma unroll
+            for (int k = 0; k < SPT; k++) {
+                const int li = tid + k * NT;
+                if (li < n_own) {
+                    T h[3], Pv[3];
+                    field(B, li, mk[k], h);
+                    const T *Sp = Pin[k];
+                    Pv[0] = h[1] * Sp[2] - h[2] * Sp[1];
+                    Pv[1] = h[2] * Sp[0] - h[0] * Sp[2];
+                    Pv[2] = h[0] * Sp[1] - h[1] * Sp[0];
+                    double v[3];
+#pragma unroll
+                    for (int c = 0; c < 3; c++) {
+                        acc[k][c] += f1 * (dt * Pv[c]);
+                        v[c] = S[k][c] + (double)acc[k][c];
+                    }
+                    normalise(v);
+#pragma unroll
+                    for (int c = 0; c < 3; c++) S[k][c] = v[c];
+                }
+            }
+            if (!fix) {
+                publishA();
+                cl_sync();
+                continue;
+            }
+            // ---- energy correction
+            if (sizeof(T) == 4) {
+                cl_sync();      // stage-4 reads of B finish before D (over A and B) is written
+                publishD();
+            } else {
+                publishA();
+            }
+            cl_sync();
+            double sig = 0.0, e1 = 0.0;
+#pragma unroll
+            for (int k = 0; k < SPT; k++) {
+                const int li = tid + k * NT;
+                if (li < n_own) {
+                    double h[3], Pv[3];
+                    if (sizeof(T) == 8) {
+                        T ht[3];
+                        field(A, li, mk[k], ht);
+                        h[0] = ht[0]; h[1] = ht[1]; h[2] = ht[2];
+                    } else {
+                        field64(li, (double)mk[k], h);
+                    }
+                    Pv[0] = h[1] * S[k][2] - h[2] * S[k][1];
+                    Pv[1] = h[2] * S[k][0] - h[0] * S[k][2];
+                    Pv[2] = h[0] * S[k][1] - h[1] * S[k][0];
+                    sig += Pv[0] * Pv[0] + Pv[1] * Pv[1] + Pv[2] * Pv[2];
+                    e1 += S[k][0] * h[0] + S[k][1] * h[1] + S[k][2] * h[2] - hz * S[k][2];
+#pragma unroll
+                    for (int c = 0; c < 3; c++) acc[k][c] = T(Pv[c]);
+                }
+            }
+            double v3[3] = {eref, sig, e1};
+            cluster_sum(v3, 3);
+            const double Eref = (sizeof(T) == 8 && per_step) ? 0.5 * v3[0] : E0;
+            const double E1 = 0.5 * v3[2];
+            double scale = (Eref - E1) / v3[1];
+            if (!(v3[1] > 0.0)) {
+                scale = 0.0;
+                if (rank == 0 && tid == 0) atomicOr(J.status, 1 << kStatusBadSigma);
+            }
+            if (rank == 0 && tid == 0) {
+                const double d = fabs(((sizeof(T) == 8 && per_step) ? Eref : E1) - E0);
+                drift = d > drift ? d : drift;
+            }
+#pragma unroll
+            for (int k = 0; k < SPT; k++) {
+                const int li = tid + k * NT;
+                if (li < n_own) {
+                    const double Pv[3] = {(double)acc[k][0], (double)acc[k][1], (double)acc[k][2]};
+                    double v[3];
+                    v[0] = S[k][0] + scale * (S[k][1] * Pv[2] - S[k][2] * Pv[1]);
+                    v[1] = S[k][1] + scale * (S[k][2] * Pv[0] - S[k][0] * Pv[2]);
+                    v[2] = S[k][2] + scale * (S[k][0] * Pv[1] - S[k][1] * Pv[0]);
+                    normalise(v);
+#pragma unroll
+                    for (int c = 0; c < 3; c++) S[k][c] = v[c];
+                }
+            }
+            publishA();   // the reduction's cluster barrier ordered every read of A / D before this
+            cl_sync();
+        }
+        record(r);
+    }
+
+    double *stw = J.state + (size_t)smp * 3 * N;
+#pragma unroll
+    for (int k = 0; k < SPT; k++) {
+        const int li = tid + k * NT;
+        if (li < n_own)
+#pragma unroll
+            for (int c = 0; c < 3; c++) stw[c * N + base + li] = S[k][c];
+    }
+    if (J.rec_end >= J.n_rec) {
+        if (sizeof(T) == 4) {
+            cl_sync();
+            publishD();
+            cl_sync();
+        }
+        const double Ef = energy();
+        if (rank == 0 && tid == 0) {
+            J.stats[smp * 4 + 1] = Ef;
+            J.stats[smp * 4 + 2] = E0;
+        }
+    }
+    if (rank == 0 && tid == 0) J.stats[smp * 4 + 0] = drift;
+    cl_sync();   // no CTA leaves while others may still touch its shared memory
+}
+
+template <typename T, int SPT, int ZT>
+cudaError_t launch_cluster_t(const ClusterParams &P, const RKJob &J, int threads, size_t smem,
+                             cudaStream_t st)
+{
+    auto k = rk_cluster_kernel<T, SPT, ZT>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    if (P.CS > 8) {
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e != cudaSuccess) return e;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(J.n_samples * P.CS, 1, 1);
+    cfg.blockDim = dim3(threads, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = P.CS;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k, P, J);
+}
+
+template <typename T, int SPT>
+cudaError_t launch_cluster_spt(const ClusterParams &P, const RKJob &J, int threads, size_t smem,
+                               cudaStream_t st)
+{
+    switch (P.ZT) {
+    case 4: return launch_cluster_t<T, SPT, 4>(P, J, threads, smem, st);
+    case 8: return launch_cluster_t<T, SPT, 8>(P, J, threads, smem, st);
+    case 12: return launch_cluster_t<T, SPT, 12>(P, J, threads, smem, st);
+    case 18: return launch_cluster_t<T, SPT, 18>(P, J, threads, smem, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+template <typename T>
+cudaError_t launch_cluster_prec(const ClusterParams &P, const RKJob &J, int spt, int threads,
+                                size_t smem, cudaStream_t st)
+{
+    switch (spt) {
+    case 1: return launch_cluster_spt<T, 1>(P, J, threads, smem, st);
+    case 2: return launch_cluster_spt<T, 2>(P, J, threads, smem, st);
+    case 4: return launch_cluster_spt<T, 4>(P, J, threads, smem, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace smd

@@ -135,6 +135,82 @@ def test_fp32_form_energy_and_spectrum_error(ctx):
     assert r32.report["drift_max"] <= 1e-8, r32.report
 
 
+@pytest.fixture
+def cluster_size(monkeypatch):
+    """Force the number of CTAs a sample is spread over (SMD_CLUSTER_CTAS)."""
+    def set_(cs):
+        monkeypatch.setenv("SMD_CLUSTER_CTAS", str(cs))
+    return set_
+
+
+@pytest.mark.parametrize("cs", [1, 2, 4, 8])
+@pytest.mark.parametrize("name", ["traj_square_xxz_h_vac", "traj_triang_j1j2", "traj_kagome",
+                                  "traj_hexagn"])
+def test_cluster_kernel_200_steps_per_spin(ctx, cluster_size, cs, name):
+    """The cluster kernel (sample split over cs CTAs, halo exchange through
+    distributed shared memory) keeps the reference's per-spin parity."""
+    cluster_size(cs)
+    s, d = load_golden(name)
+    lat, lid = _upload(ctx, s)
+    n = int(d["n"])
+    imp = None if "imp" not in d else np.tile(d["imp"], (n, 1))
+    fin = ctx.evolve(lid, d["spins0"][:n], s.dtm, s.ntm - 1, imp=imp)
+    assert np.max(np.abs(fin - d["final"])) <= SPIN_TOL
+
+
+@pytest.mark.parametrize("cs", [2, 4])
+def test_cluster_kernel_spectrum(ctx, cluster_size, cs):
+    cluster_size(cs)
+    s, d = load_golden("spec_kagome")
+    lat, lid = _upload(ctx, s)
+    qid = ctx.qset(lid, use_grid=True)
+    n = int(d["n"])
+    r = ctx.run(lid, qid, d["spins0"][:n], s.dtm, s.ntm, win=d["window"])
+    ref = d["spec_sum"] / n
+    assert np.max(np.abs(r.spec - ref)) <= SPEC_TOL * np.max(np.abs(ref))
+    assert np.max(np.abs(r.final - d["final"])) <= SPIN_TOL
+
+
+@pytest.mark.parametrize("cs", [1, 2, 4])
+def test_cluster_fp32_form_tracks_fp64(ctx, cluster_size, cs):
+    """FP32 precision form on a cluster: spectrum within 1e-3 (rel-L2) of the
+    FP64 form, energy drift within 1e-8 per site."""
+    cluster_size(cs)
+    s = SMDSettings(geom="square", L=32, J2=0.55, JX=0.1, zlamb1=0.9, zlamb2=0.9, h=0.3,
+                    imp_ratio=0.05, dtm=0.01, ntm=128, NMeas=4000)
+    lat, lid = _upload(ctx, s)
+    qid = ctx.qset(lid)
+    spins, imp = smp.make_samples(s, 4, "stripe", 0.1, 5)
+    impr = np.tile(imp[0], (4, 1))
+    win = smd.window("hann1", 128)
+    r64 = ctx.run(lid, qid, spins, s.dtm, 128, stride=4, win=win, imp=impr)
+    r32 = ctx.run(lid, qid, spins, s.dtm, 128, stride=4, win=win, imp=impr,
+                  precision=_lib.SMD_FP32, fix_every=16)
+    rel = np.linalg.norm(r32.spec - r64.spec) / np.linalg.norm(r64.spec)
+    assert rel <= 1e-3, rel
+    assert r32.report["drift_max"] <= 1e-8 and r32.report["drift_final"] <= 1e-8
+
+
+def test_cluster_vacancies_match_oracle(ctx, oracle_mod, cluster_size):
+    """Vacancy disorder through the masked cluster kernel against the oracle."""
+    cluster_size(2)
+    s = SMDSettings(geom="square", L=16, J2=0.55, JX=0.1, zlamb1=0.9, zlamb2=0.9, h=0.3,
+                    imp_ratio=0.05, dtm=0.01, ntm=24, NMeas=2000)
+    lat, lid = _upload(ctx, s)
+    qid = ctx.qset(lid)
+    spins, imp = smp.make_samples(s, 2, "stripe", 0.2, 8)
+    impr = np.tile(imp[0], (2, 1))
+    r = ctx.run(lid, qid, spins, s.dtm, 24, stride=3, imp=impr)
+    m = oracle_mod.Model(s, oracle_mod.make_lattice(s.geom, s.L), imp[0])
+    acc = 0.0
+    for k in range(2):
+        o = oracle_mod.dyn_spectrum(m, spins[k], s.dtm, 24, stride=3)
+        acc = acc + o["spec"]
+        assert np.max(np.abs(r.final[k] - o["final"])) <= SPIN_TOL
+    acc /= 2
+    assert np.max(np.abs(r.spec - acc)) <= SPEC_TOL * np.max(np.abs(acc))
+
+
 def test_invalid_jobs_fail_loudly(ctx):
     s = SMDSettings(geom="square", L=8, J2=0.6, dtm=0.01, ntm=16)
     lat, lid = _upload(ctx, s)
