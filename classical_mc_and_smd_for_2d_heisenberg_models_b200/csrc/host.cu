@@ -91,6 +91,12 @@ struct QSet {
     FFTPlan gplan{};
     DevBuf tw64, tw32;        // grid twiddles
     DevBuf phase64, phase32;  // [N][n_list] complex
+    // tensor-core operand of the FP32 form: rows 2l / 2l + 1 hold
+    // scale cos(q_l . r_k) / -scale sin(q_l . r_k), split into bf16 high and
+    // low parts, row pitch kp
+    int kp = 0;
+    DevBuf bhi, blo;
+    CUtensorMap map_bhi{}, map_blo{};
 };
 
 struct Plan {
@@ -115,6 +121,11 @@ struct smd_ctx {
     DevBuf state, s0, imp, snap[2], series, qss, stats, e0, status, win, acc_tmp, in_tmp, out_tmp;
     int launches = 0;
     std::vector<cudaEvent_t> tev;   // timing events, reused across calls
+    // bf16 high / low parts of one chunk's snapshot rows and their maps
+    DevBuf ahi, alo;
+    CUtensorMap map_ahi{}, map_alo{};
+    const void *map_a_base = nullptr;
+    int map_a_rows = 0, map_a_kp = 0;
 };
 
 namespace {
@@ -153,6 +164,23 @@ bool make_plan(int n, FFTPlan &p)
         }
     }
     return m == 1;
+}
+
+// bf16 bits of x, rounded to nearest even (x finite)
+uint16_t bf16_bits(float x)
+{
+    uint32_t u;
+    std::memcpy(&u, &x, 4);
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+}
+
+float bf16_value(uint16_t h)
+{
+    const uint32_t u = (uint32_t)h << 16;
+    float x;
+    std::memcpy(&x, &u, 4);
+    return x;
 }
 
 // exp(-2 pi i j / n) for j < n, accurate to one rounding
@@ -437,6 +465,26 @@ extern "C" int smd_qset_upload(smd_ctx *ctx, int lattice_id, int use_grid, int n
         CK(cudaMemcpy(Q->phase64.p, ph.data(), ph.size() * sizeof(double), cudaMemcpyHostToDevice), "H2D");
         CK(Q->phase32.ensure(pf.size() * sizeof(float)), "cudaMalloc");
         CK(cudaMemcpy(Q->phase32.p, pf.data(), pf.size() * sizeof(float), cudaMemcpyHostToDevice), "H2D");
+        // split-bf16 operand of the tensor-core projection, [2 n_list][kp]
+        const int kp = tc_kpitch(N);
+        Q->kp = kp;
+        std::vector<uint16_t> bh((size_t)2 * n_list * kp, 0), bl((size_t)2 * n_list * kp, 0);
+        for (int l = 0; l < n_list; l++)
+            for (int k = 0; k < N; k++)
+                for (int part = 0; part < 2; part++) {
+                    const double x = ph[2 * ((size_t)k * n_list + l) + part];
+                    const uint16_t hi = bf16_bits((float)x);
+                    const uint16_t lo = bf16_bits((float)(x - (double)bf16_value(hi)));
+                    bh[((size_t)2 * l + part) * kp + k] = hi;
+                    bl[((size_t)2 * l + part) * kp + k] = lo;
+                }
+        CK(Q->bhi.ensure(bh.size() * 2), "cudaMalloc");
+        CK(Q->blo.ensure(bl.size() * 2), "cudaMalloc");
+        CK(cudaMemcpy(Q->bhi.p, bh.data(), bh.size() * 2, cudaMemcpyHostToDevice), "H2D");
+        CK(cudaMemcpy(Q->blo.p, bl.data(), bl.size() * 2, cudaMemcpyHostToDevice), "H2D");
+        if (!make_bf16_map(&Q->map_bhi, Q->bhi.p, 2 * n_list, kp, tc_bn()) ||
+            !make_bf16_map(&Q->map_blo, Q->blo.p, 2 * n_list, kp, tc_bn()))
+            return fail(ctx, SMD_ECUDA, "qset: tensor map encoding failed");
     }
     const int id = ctx->next_id++;
     ctx->qsets[id] = std::move(Q);
@@ -781,10 +829,30 @@ int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const do
                                     ctx->series.p, Q, ctx->s_proj), "grid projection");
                 ctx->launches++;
             }
-            if (Qs.n_list > 0) {
+            if (Qs.n_list > 0 && g.prec == SMD_FP32) {
+                // split-BF16 tensor-core projection of the chunk's rows
+                const int rows = Ww * R * 3, kp = Qs.kp;
+                CK(ctx->ahi.ensure((size_t)W * R * 3 * kp * 2), "cudaMalloc");
+                CK(ctx->alo.ensure((size_t)W * R * 3 * kp * 2), "cudaMalloc");
+                if (ctx->map_a_base != ctx->ahi.p || ctx->map_a_rows != rows || ctx->map_a_kp != kp) {
+                    if (!make_bf16_map(&ctx->map_ahi, ctx->ahi.p, rows, kp, tc_bm()) ||
+                        !make_bf16_map(&ctx->map_alo, ctx->alo.p, rows, kp, tc_bm()))
+                        return fail(ctx, SMD_ECUDA, "tensor map encoding failed");
+                    ctx->map_a_base = ctx->ahi.p;
+                    ctx->map_a_rows = rows;
+                    ctx->map_a_kp = kp;
+                }
+                CK(launch_split_bf16(ctx->snap[b].as<float>(), rows, N, kp, ctx->ahi.p, ctx->alo.p,
+                                     ctx->s_proj), "bf16 split");
+                CK(launch_list_proj_tc(ctx->map_ahi, ctx->map_alo, Qs.map_bhi, Qs.map_blo, rows, kp,
+                                       R, re - rb, rb, n_rec, Qs.n_list, ctx->series.p, Q,
+                                       Qs.G * Qs.G, ctx->status.as<int>(), ctx->s_proj),
+                   "tensor-core list projection");
+                ctx->launches += 2;
+            } else if (Qs.n_list > 0) {
                 CK(launch_list_proj_simt(ctx->snap[b].p, g.prec, Ww, R, re - rb, N, rb, n_rec,
-                                         g.prec == SMD_FP64 ? Qs.phase64.p : Qs.phase32.p,
-                                         Qs.n_list, ctx->series.p, Q, Qs.G * Qs.G, ctx->s_proj),
+                                         Qs.phase64.p, Qs.n_list, ctx->series.p, Q, Qs.G * Qs.G,
+                                         ctx->s_proj),
                    "list projection");
                 ctx->launches++;
             }
@@ -836,6 +904,7 @@ int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const do
         rep->rk_launches = rk_launches;
         rep->site_steps = (double)N * (double)(n_rec - 1) * job->stride * job->n_samples;
     }
+    if (st & 4) return fail(ctx, SMD_ETIMEOUT, "tensor-core projection: a bounded wait expired");
     if (st) return fail(ctx, SMD_ECUDA, "a sample reached a zero correction denominator (sigma = 0)");
     return SMD_OK;
 }

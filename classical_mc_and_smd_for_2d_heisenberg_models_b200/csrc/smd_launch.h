@@ -1,6 +1,8 @@
 // smd_launch.h -- host-side declarations of the kernel launchers.
 #pragma once
 
+#include <cuda.h>
+
 #include "smd_device.cuh"
 
 namespace smd {
@@ -26,5 +28,17 @@ cudaError_t launch_time_fft(const void *series, int precision, int W, int Q, con
 cudaError_t launch_aos_to_soa(const double *in, double *out, int W, int N, cudaStream_t st);
 cudaError_t launch_soa_to_aos(const double *in, double *out, int W, int N, cudaStream_t st);
 cudaError_t launch_sum_rows(const double *rows, int W, int n, double *out, cudaStream_t st);
+
+// tensor-core list projection (proj_tc.cu)
+bool make_bf16_map(CUtensorMap *map, const void *base, int rows, int kp, int box_rows);
+int tc_kpitch(int N);
+int tc_bn();
+int tc_bm();
+cudaError_t launch_split_bf16(const float *x, int rows, int N, int kp, void *hi, void *lo,
+                              cudaStream_t st);
+cudaError_t launch_list_proj_tc(const CUtensorMap &Ah, const CUtensorMap &Al, const CUtensorMap &Bh,
+                                const CUtensorMap &Bl, int M, int kp, int R, int nrec_chunk,
+                                int rec_begin, int n_rec_total, int Lq, void *series, int Q,
+                                int qoff, int *status, cudaStream_t st);
 
 }  // namespace smd
