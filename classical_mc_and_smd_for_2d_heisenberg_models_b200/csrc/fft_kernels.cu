@@ -18,6 +18,8 @@
 // of one component, loops over every sample of the wave and keeps the sum
 // over samples in registers, so the accumulation needs no atomics and is
 // deterministic.
+#include <cuda.h>
+
 #include "smd_device.cuh"
 
 namespace smd {
@@ -87,12 +89,17 @@ __device__ __forceinline__ void stockham_stage(cplx<T> *buf, int n, int nseq, in
                                                int Ns, const cplx<T> *tw)
 {
     const int m = n / R, nb = nseq * m;
+    // Consecutive threads take consecutive elements: along a sequence when
+    // its elements are adjacent (es == 1), across sequences otherwise, so
+    // shared-memory accesses stay free of bank conflicts.
+    const bool qfast = es != 1;
     cplx<T> v[NB][R];
 #pragma unroll
     for (int u = 0; u < NB; u++) {
         const int b = threadIdx.x + u * blockDim.x;
         if (b < nb) {
-            const int q = b / m, j = b - q * m;
+            const int q = qfast ? b % nseq : b / m;
+            const int j = qfast ? b / nseq : b - q * m;
 #pragma unroll
             for (int r = 0; r < R; r++) v[u][r] = buf[q * ss + (j + r * m) * es];
         }
@@ -103,7 +110,9 @@ __device__ __forceinline__ void stockham_stage(cplx<T> *buf, int n, int nseq, in
     for (int u = 0; u < NB; u++) {
         const int b = threadIdx.x + u * blockDim.x;
         if (b < nb) {
-            const int q = b / m, j = b - q * m, k = j % Ns;
+            const int q = qfast ? b % nseq : b / m;
+            const int j = qfast ? b / nseq : b - q * m;
+            const int k = j % Ns;
 #pragma unroll
             for (int r = 1; r < R; r++) v[u][r] = cmul(v[u][r], tw[((r * k) * tstep) % n]);
             dft_small<T, R>(v[u], tw, n);
@@ -277,7 +286,7 @@ __global__ void __launch_bounds__(256) list_proj_simt_kernel(
 // into acc[c][q][n_rec] (added to what acc holds).
 template <typename T>
 __global__ void __launch_bounds__(1024) time_fft_kernel(
-    const cplx<T> *__restrict__ series, int W, int Q, int QT, FFTPlan plan,
+    const cplx<T> *__restrict__ series, int W, int Q, int Qp, int QT, FFTPlan plan,
     const cplx<T> *__restrict__ tw_g, const double *__restrict__ win, double *__restrict__ acc,
     int use_scratch)
 {
@@ -295,10 +304,10 @@ __global__ void __launch_bounds__(1024) time_fft_kernel(
     const int total = qt * n;
     const double inv_n = 1.0 / n;
     for (int s = 0; s < W; s++) {
-        const cplx<T> *src = series + ((size_t)s * 3 + c) * n * Q + q0;
+        const cplx<T> *src = series + ((size_t)s * 3 + c) * n * Qp + q0;
         for (int e = threadIdx.x; e < total; e += blockDim.x) {
             const int qq = e % qt, t = e / qt;
-            const cplx<T> v = src[(size_t)t * Q + qq];
+            const cplx<T> v = src[(size_t)t * Qp + qq];
             const T w = T(win[t]);
             buf[qq * n + t] = {w * v.x, w * v.y};
         }
@@ -319,6 +328,98 @@ __global__ void __launch_bounds__(1024) time_fft_kernel(
     for (int u = 0; u < MAXA; u++) {
         const int e = threadIdx.x + u * blockDim.x;
         if (e < total) out[e] += a[u];
+    }
+}
+
+// Same transform fed by TMA: each sample's [n][QT] tile (all records, QT
+// consecutive q) arrives as n / box_rows 2D boxes on one mbarrier, so the
+// whole tile is in flight at once.  The tile stays in the [t][q] order it
+// lands in (sequence stride 1, element stride QT).  Waits are bounded; on
+// expiry the kernel records bit 8 in *status and stops.
+template <typename T>
+__global__ void __launch_bounds__(1024) time_fft_tma_kernel(
+    const __grid_constant__ CUtensorMap smap, int W, int Q, int QT, int box_rows, FFTPlan plan,
+    const cplx<T> *__restrict__ tw_g, const double *__restrict__ win, double *__restrict__ acc,
+    int use_scratch, int *status)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const int n = plan.n;
+    const int ntile = (Q + QT - 1) / QT;
+    const int c = blockIdx.x / ntile, q0 = (blockIdx.x % ntile) * QT;
+    cplx<T> *buf = reinterpret_cast<cplx<T> *>(smem_raw);
+    const size_t tile = (size_t)QT * n;
+    cplx<T> *scratch = use_scratch ? buf + tile : nullptr;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + (use_scratch ? 2 : 1) * tile * sizeof(cplx<T>));
+    const uint32_t bar_a = (uint32_t)__cvta_generic_to_shared(bar);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    constexpr int MAXA = FFTCap<T>::v;
+    double a[MAXA];
+#pragma unroll
+    for (int u = 0; u < MAXA; u++) a[u] = 0.0;
+    const int total = QT * n;
+    const double inv_n = 1.0 / n;
+    const unsigned bytes = (unsigned)(tile * sizeof(cplx<T>));
+    bool ok = true;
+    for (int s = 0; s < W && ok; s++) {
+        if (threadIdx.x == 0) {
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a),
+                         "r"(bytes)
+                         : "memory");
+            for (int b = 0; b < n / box_rows; b++) {
+                const uint32_t dst =
+                    (uint32_t)__cvta_generic_to_shared(buf + (size_t)b * box_rows * QT);
+                asm volatile(
+                    "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes "
+                    "[%0], [%1, {%3, %4}], [%2];" ::"r"(dst),
+                    "l"(reinterpret_cast<uint64_t>(&smap)), "r"(bar_a), "r"(2 * q0),
+                    "r"((s * 3 + c) * n + b * box_rows)
+                    : "memory");
+            }
+        }
+        uint32_t done = 0;
+        for (unsigned it = 0; it < (1u << 26) && !done; it++) {
+            asm volatile(
+                "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                " selp.u32 %0, 1, 0, p;\n}\n"
+                : "=r"(done)
+                : "r"(bar_a), "r"((unsigned)(s & 1))
+                : "memory");
+        }
+        if (!done) {
+            if (threadIdx.x == 0) atomicOr(status, 8);
+            ok = false;
+            break;
+        }
+        for (int e = threadIdx.x; e < total; e += blockDim.x) {
+            const T w = T(win[e / QT]);
+            cplx<T> v = buf[e];
+            buf[e] = {w * v.x, w * v.y};
+        }
+        __syncthreads();
+        smem_fft<T>(buf, n, QT, 1, QT, plan.radix, plan.nst, tw_g, scratch);
+#pragma unroll
+        for (int u = 0; u < MAXA; u++) {
+            const int e = threadIdx.x + u * blockDim.x;
+            if (e < total) {
+                const double x = (double)buf[e].x, y = (double)buf[e].y;
+                a[u] += (x * x + y * y) * inv_n;
+            }
+        }
+        __syncthreads();
+    }
+    if (!ok) return;
+#pragma unroll
+    for (int u = 0; u < MAXA; u++) {
+        const int e = threadIdx.x + u * blockDim.x;
+        if (e < total) {
+            const int om = e / QT, qq = e - om * QT;
+            if (q0 + qq < Q) acc[((size_t)c * Q + q0 + qq) * n + om] += a[u];
+        }
     }
 }
 
@@ -449,24 +550,52 @@ size_t time_fft_smem(int n, int qt, int precision, const FFTPlan &p)
     return b;
 }
 
-cudaError_t launch_time_fft(const void *series, int precision, int W, int Q, const FFTPlan &plan,
-                            const void *tw, const double *win, double *acc, cudaStream_t st)
+// Rows per TMA box for the time transform: the largest divisor of n up to
+// 256 whose box starts on a 128-byte boundary of the tile; 0 when none.
+int time_fft_box_rows(int n, int qt, int precision)
+{
+    const size_t cs = precision == 0 ? sizeof(cplx<double>) : sizeof(cplx<float>);
+    if ((size_t)qt * cs < 16) return 0;
+    for (int d = n < 256 ? n : 256; d >= 1; d--)
+        if (n % d == 0 && ((size_t)d * qt * cs) % 128 == 0) return d;
+    return 0;
+}
+
+cudaError_t launch_time_fft(const void *series, const CUtensorMap *smap, int precision, int W, int Q,
+                            int Qp, const FFTPlan &plan, const void *tw, const double *win,
+                            double *acc, int *status, cudaStream_t st)
 {
     const int n = plan.n;
     const int qt = time_fft_qt(n, precision);
-    const size_t smem = time_fft_smem(n, qt, precision, plan);
+    size_t smem = time_fft_smem(n, qt, precision, plan);
     const int threads = fft_threads(qt * n, precision);
     const int ntile = (Q + qt - 1) / qt;
     const int gen = plan_generic(plan) ? 1 : 0;
+    const int box = smap ? time_fft_box_rows(n, qt, precision) : 0;
+    if (box) {
+        smem += 16;   // the mbarrier
+        if (precision == 0) {
+            auto k = time_fft_tma_kernel<double>;
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            k<<<3 * ntile, threads, smem, st>>>(*smap, W, Q, qt, box, plan,
+                                                (const cplx<double> *)tw, win, acc, gen, status);
+        } else {
+            auto k = time_fft_tma_kernel<float>;
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            k<<<3 * ntile, threads, smem, st>>>(*smap, W, Q, qt, box, plan,
+                                                (const cplx<float> *)tw, win, acc, gen, status);
+        }
+        return cudaGetLastError();
+    }
     if (precision == 0) {
         auto k = time_fft_kernel<double>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k<<<3 * ntile, threads, smem, st>>>((const cplx<double> *)series, W, Q, qt, plan,
+        k<<<3 * ntile, threads, smem, st>>>((const cplx<double> *)series, W, Q, Qp, qt, plan,
                                             (const cplx<double> *)tw, win, acc, gen);
     } else {
         auto k = time_fft_kernel<float>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k<<<3 * ntile, threads, smem, st>>>((const cplx<float> *)series, W, Q, qt, plan,
+        k<<<3 * ntile, threads, smem, st>>>((const cplx<float> *)series, W, Q, Qp, qt, plan,
                                             (const cplx<float> *)tw, win, acc, gen);
     }
     return cudaGetLastError();

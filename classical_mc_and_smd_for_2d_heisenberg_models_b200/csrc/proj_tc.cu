@@ -309,6 +309,22 @@ bool make_bf16_map(CUtensorMap *map, const void *base, int rows, int kp, int box
               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+bool make_real_map(CUtensorMap *map, const void *base, int precision, size_t inner, size_t rows,
+                   int box_inner, int box_rows)
+{
+    auto fn = tc::encode_fn();
+    if (!fn) return false;
+    const size_t es = precision == 0 ? 8 : 4;
+    cuuint64_t dims[2] = {(cuuint64_t)inner, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)(inner * es)};
+    cuuint32_t box[2] = {(cuuint32_t)box_inner, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    return fn(map, precision == 0 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+              2, const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 int tc_kpitch(int N) { return (N + 63) / 64 * 64; }
 int tc_bn() { return tc::BN; }
 int tc_bm() { return tc::BM; }

@@ -23,14 +23,19 @@ cudaError_t launch_list_proj_simt(const void *snap, int precision, int W, int R,
                                   void *series, int Q, int qoff, cudaStream_t st);
 int time_fft_qt(int n, int precision);
 size_t time_fft_smem(int n, int qt, int precision, const FFTPlan &p);
-cudaError_t launch_time_fft(const void *series, int precision, int W, int Q, const FFTPlan &plan,
-                            const void *tw, const double *win, double *acc, cudaStream_t st);
+int time_fft_box_rows(int n, int qt, int precision);
+cudaError_t launch_time_fft(const void *series, const CUtensorMap *smap, int precision, int W, int Q,
+                            int Qp, const FFTPlan &plan, const void *tw, const double *win,
+                            double *acc, int *status, cudaStream_t st);
 cudaError_t launch_aos_to_soa(const double *in, double *out, int W, int N, cudaStream_t st);
 cudaError_t launch_soa_to_aos(const double *in, double *out, int W, int N, cudaStream_t st);
 cudaError_t launch_sum_rows(const double *rows, int W, int n, double *out, cudaStream_t st);
 
 // tensor-core list projection (proj_tc.cu)
 bool make_bf16_map(CUtensorMap *map, const void *base, int rows, int kp, int box_rows);
+// row-major [rows][inner] matrix of FP32 (precision 1) or FP64 (0) values
+bool make_real_map(CUtensorMap *map, const void *base, int precision, size_t inner, size_t rows,
+                   int box_inner, int box_rows);
 int tc_kpitch(int N);
 int tc_bn();
 int tc_bm();
