@@ -6,15 +6,17 @@
 // fit the context's HBM budget.  Within a wave the records are produced in
 // chunks of R records:
 //
-//   stream rk   : RK kernel, one CTA per sample, writes the chunk's spin
-//                 snapshots into one of two snapshot buffers
+//   stream rk   : RK kernel (one CTA, or one cluster of CTAs, per sample)
+//                 writes the chunk's spin snapshots into one of two
+//                 snapshot buffers
 //   stream proj : grid projection (2D FFT) and list projection of the chunk,
-//                 writing S(q,t) into the wave's time series
+//                 writing the windowed w[t] S(q,t) into the wave's q-blocked
+//                 time series (series_off)
 //
 // so the projection of chunk c overlaps the integration of chunk c+1 on the
 // SMs the RK kernel leaves free.  After the last chunk the time-FFT kernel
-// windows, transforms and squares every series and adds the sum over the
-// wave's samples into the job's accumulator.
+// transforms and squares every series and adds the sum over the wave's
+// samples into the job's accumulator.
 #include "../../include/smd_b200.h"
 #include "rk_cluster.cuh"
 #include "smd_launch.h"
@@ -126,11 +128,6 @@ struct smd_ctx {
     CUtensorMap map_ahi{}, map_alo{};
     const void *map_a_base = nullptr;
     int map_a_rows = 0, map_a_kp = 0;
-    // the series map of the TMA-fed time transform
-    CUtensorMap smap{};
-    const void *smap_base = nullptr;
-    size_t smap_rows = 0;
-    int smap_prec = -1, smap_qp = 0, smap_box = 0, smap_qt = 0;
 };
 
 namespace {
@@ -512,7 +509,7 @@ struct JobGeom {
     Lattice *L;
     QSet *Qs;
     Plan *tp;
-    int N, Q, Qp, n_rec, prec, R, W, waves;   // Qp: series row pitch (multiple of 4)
+    int N, Q, nqb, n_rec, prec, R, W, waves;   // nqb: q blocks of the series layout
     size_t elem, celem;
     ClusterTab *ctab = nullptr;   // cluster kernel partition (null: single-CTA kernel)
     int spt = 0, threads = 0;
@@ -699,9 +696,9 @@ int prepare(smd_ctx *ctx, const smd_job_desc *job, JobGeom &g)
     g.Qs = qi->second.get();
     g.N = g.L->N;
     g.Q = g.Qs->Q;
-    g.Qp = (g.Q + 3) / 4 * 4;
     g.n_rec = job->n_rec;
     g.prec = job->precision;
+    g.nqb = (g.Q + series_qblock(g.prec) - 1) / series_qblock(g.prec);
     choose_cluster(ctx, g, job->n_samples);
     if (!g.ctab && g.N > rk_max_sites(g.prec))
         return fail(ctx, SMD_EINVAL, "job: N exceeds the single-CTA capacity of this form");
@@ -717,16 +714,14 @@ int prepare(smd_ctx *ctx, const smd_job_desc *job, JobGeom &g)
         pi = ctx->tplans.emplace(g.n_rec, std::move(P)).first;
     }
     g.tp = pi->second.get();
-    const int qt = time_fft_qt(g.n_rec, g.prec);
-    const size_t fft_cap = g.prec == SMD_FP64 ? 8192 : 16384;
-    if ((size_t)qt * g.n_rec > fft_cap || time_fft_smem(g.n_rec, qt, g.prec, g.tp->p) > 200 * 1024)
+    if (!time_fft_fits(g.n_rec, g.prec, g.tp->p))
         return fail(ctx, SMD_EINVAL, "job: n_rec too long for the shared-memory time transform");
     // chunk of records per RK launch
     g.R = std::min(g.n_rec, 64);
     // per-sample device bytes
     const size_t N = g.N;
     const size_t per = 2 * 3 * N * sizeof(double) + N + 2 * (size_t)g.R * 3 * N * g.elem +
-                       3 * (size_t)g.n_rec * g.Qp * g.celem + (size_t)g.n_rec * sizeof(double) +
+                       3 * (size_t)g.n_rec * g.nqb * 16 + (size_t)g.n_rec * sizeof(double) +
                        5 * sizeof(double);
     const size_t fixed = 3 * (size_t)g.Q * g.n_rec * sizeof(double) + (64u << 20);
     if (ctx->budget <= fixed + per) return fail(ctx, SMD_ENOMEM_ADMIT, "job: one sample exceeds the HBM budget");
@@ -743,7 +738,7 @@ int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const do
                const double *d_win, double *d_spec_sum, double *d_qss_sum, double *d_final,
                smd_report *rep)
 {
-    const int N = g.N, Q = g.Q, Qp = g.Qp, n_rec = g.n_rec, R = g.R, W = g.W;
+    const int N = g.N, Q = g.Q, nqb = g.nqb, n_rec = g.n_rec, R = g.R, W = g.W;
     Lattice &L = *g.L;
     QSet &Qs = *g.Qs;
     CK(ctx->state.ensure((size_t)W * 3 * N * sizeof(double)), "cudaMalloc state");
@@ -751,7 +746,7 @@ int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const do
     CK(ctx->imp.ensure((size_t)W * N), "cudaMalloc imp");
     for (int b = 0; b < 2; b++)
         CK(ctx->snap[b].ensure((size_t)W * R * 3 * N * g.elem), "cudaMalloc snap");
-    CK(ctx->series.ensure((size_t)W * 3 * n_rec * Qp * g.celem), "cudaMalloc series");
+    CK(ctx->series.ensure((size_t)W * 3 * n_rec * nqb * 16), "cudaMalloc series");
     CK(ctx->qss.ensure((size_t)W * n_rec * sizeof(double)), "cudaMalloc qss");
     CK(ctx->stats.ensure((size_t)W * 4 * sizeof(double)), "cudaMalloc stats");
     CK(ctx->e0.ensure((size_t)W * sizeof(double)), "cudaMalloc e0");
@@ -831,8 +826,8 @@ int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const do
                 const double scale = std::sqrt(1.0 / ((double)Qs.G * Qs.G));   // subrouts.cpp:8343
                 CK(launch_grid_proj(ctx->snap[b].p, g.prec, N, Ww, R, re - rb, rb, n_rec,
                                     L.grid_map.as<int>(), Qs.gplan,
-                                    g.prec == SMD_FP64 ? Qs.tw64.p : Qs.tw32.p, scale,
-                                    ctx->series.p, Qp, ctx->s_proj), "grid projection");
+                                    g.prec == SMD_FP64 ? Qs.tw64.p : Qs.tw32.p, scale, d_win,
+                                    ctx->series.p, nqb, ctx->s_proj), "grid projection");
                 ctx->launches++;
             }
             if (Qs.n_list > 0 && g.prec == SMD_FP32) {
@@ -851,13 +846,13 @@ int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const do
                 CK(launch_split_bf16(ctx->snap[b].as<float>(), rows, N, kp, ctx->ahi.p, ctx->alo.p,
                                      ctx->s_proj), "bf16 split");
                 CK(launch_list_proj_tc(ctx->map_ahi, ctx->map_alo, Qs.map_bhi, Qs.map_blo, rows, kp,
-                                       R, re - rb, rb, n_rec, Qs.n_list, ctx->series.p, Qp,
+                                       R, re - rb, rb, n_rec, Qs.n_list, d_win, ctx->series.p, nqb,
                                        Qs.G * Qs.G, ctx->status.as<int>(), ctx->s_proj),
                    "tensor-core list projection");
                 ctx->launches += 2;
             } else if (Qs.n_list > 0) {
                 CK(launch_list_proj_simt(ctx->snap[b].p, g.prec, Ww, R, re - rb, N, rb, n_rec,
-                                         Qs.phase64.p, Qs.n_list, ctx->series.p, Qp, Qs.G * Qs.G,
+                                         Qs.phase64.p, Qs.n_list, d_win, ctx->series.p, nqb, Qs.G * Qs.G,
                                          ctx->s_proj),
                    "list projection");
                 ctx->launches++;
@@ -866,32 +861,9 @@ int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const do
             CK(cudaEventRecord(ctx->ev_proj[b], ctx->s_proj), "event");
         }
         CK(cudaEventRecord(ev(nev - 2), ctx->s_proj), "event");
-        {
-            // tensor map of this wave's series for the TMA-fed transform
-            const int qt = time_fft_qt(n_rec, g.prec);
-            const int box = time_fft_box_rows(n_rec, qt, g.prec);
-            const CUtensorMap *smap = nullptr;
-            if (box) {
-                const size_t rows = (size_t)Ww * 3 * n_rec;
-                if (ctx->smap_base != ctx->series.p || ctx->smap_rows != rows ||
-                    ctx->smap_prec != g.prec || ctx->smap_qp != Qp || ctx->smap_box != box ||
-                    ctx->smap_qt != qt) {
-                    if (!make_real_map(&ctx->smap, ctx->series.p, g.prec, 2 * (size_t)Qp, rows,
-                                       2 * qt, box))
-                        return fail(ctx, SMD_ECUDA, "series tensor map encoding failed");
-                    ctx->smap_base = ctx->series.p;
-                    ctx->smap_rows = rows;
-                    ctx->smap_prec = g.prec;
-                    ctx->smap_qp = Qp;
-                    ctx->smap_box = box;
-                    ctx->smap_qt = qt;
-                }
-                smap = &ctx->smap;
-            }
-            CK(launch_time_fft(ctx->series.p, smap, g.prec, Ww, Q, Qp, g.tp->p,
-                               g.prec == SMD_FP64 ? g.tp->tw64.p : g.tp->tw32.p, d_win, d_spec_sum,
-                               ctx->status.as<int>(), ctx->s_proj), "time fft");
-        }
+        CK(launch_time_fft(ctx->series.p, g.prec, Ww, Q, nqb, g.tp->p,
+                           g.prec == SMD_FP64 ? g.tp->tw64.p : g.tp->tw32.p, d_spec_sum,
+                           ctx->status.as<int>(), ctx->s_proj), "time fft");
         CK(cudaEventRecord(ev(nev - 1), ctx->s_proj), "event");
         ctx->launches++;
         CK(cudaStreamWaitEvent(ctx->s_proj, ctx->ev_rk[(nchunks - 1) & 1], 0), "wait");

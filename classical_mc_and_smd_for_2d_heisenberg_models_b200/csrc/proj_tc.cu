@@ -15,8 +15,8 @@
 // Tile 128 x 256, K blocks of 64 bf16 (one 128-byte swizzle row).  Warp 0
 // loads A and B K-blocks with TMA (128B swizzle) into a 4-stage ring, warp 1
 // issues tcgen05.mma (M=128, N=256, K=16) from one thread, and all four warps
-// drain the accumulator with tcgen05.ld and store complex64 values straight
-// into the time series.  Every mbarrier wait is bounded: after the limit the
+// drain the accumulator with tcgen05.ld, apply the record's window weight and
+// store complex64 values straight into the q-blocked time series.  Every mbarrier wait is bounded: after the limit the
 // kernel records an error, stops issuing work, waits (bounded) for its
 // copies in flight, frees its tensor memory and returns.
 #include "smd_device.cuh"
@@ -142,7 +142,8 @@ __global__ void __launch_bounds__(128, 1) list_proj_tc_kernel(
     const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
     const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl, int M,
     int nkb, int R, int nrec_chunk, int rec_begin, int n_rec_total, int Lq,
-    cplx<float> *__restrict__ series, int Q, int qoff, int *status)
+    const double *__restrict__ win, cplx<float> *__restrict__ series, int nqb, int qoff,
+    int *status)
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *sm = reinterpret_cast<unsigned char *>(
@@ -235,17 +236,33 @@ __global__ void __launch_bounds__(128, 1) list_proj_tc_kernel(
     const int row = m0 + warp * 32 + lane;
     const int c = row % 3, slot = row / 3 % R, s = row / (3 * R);
     const bool row_ok = have && row < M && slot < nrec_chunk;
-    cplx<float> *out = series + (((size_t)s * 3 + c) * n_rec_total + rec_begin + slot) * Q + qoff;
+    // windowed series: record t of this row, q = qoff + l in blocks of two
+    const int t = rec_begin + slot;
+    const float w = row_ok ? (float)win[t] : 0.f;
+    cplx<float> *out = series + series_off<float>(s, c, 0, t, nqb, n_rec_total);
+    const size_t bstride = (size_t)n_rec_total * 2;   // elements between q blocks
     if (have) {
 #pragma unroll 1
         for (int c0 = 0; c0 < BN; c0 += 16) {
             float v[16];
             tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + c0, v);
             if (row_ok) {
+                const int l0 = (n0 + c0) / 2;
+                if ((qoff & 1) == 0 && l0 + 8 <= Lq) {
+                    // whole blocks: one 16-byte store per pair of q
 #pragma unroll
-                for (int p = 0; p < 8; p++) {
-                    const int l = (n0 + c0) / 2 + p;
-                    if (l < Lq) out[l] = {v[2 * p], v[2 * p + 1]};
+                    for (int p = 0; p < 4; p++) {
+                        const int q = qoff + l0 + 2 * p;
+                        *reinterpret_cast<float4 *>(out + (q >> 1) * bstride) =
+                            make_float4(w * v[4 * p], w * v[4 * p + 1], w * v[4 * p + 2],
+                                        w * v[4 * p + 3]);
+                    }
+                } else {
+#pragma unroll
+                    for (int p = 0; p < 8; p++) {
+                        const int l = l0 + p, q = qoff + l;
+                        if (l < Lq) out[(q >> 1) * bstride + (q & 1)] = {w * v[2 * p], w * v[2 * p + 1]};
+                    }
                 }
             }
         }
@@ -309,22 +326,6 @@ bool make_bf16_map(CUtensorMap *map, const void *base, int rows, int kp, int box
               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-bool make_real_map(CUtensorMap *map, const void *base, int precision, size_t inner, size_t rows,
-                   int box_inner, int box_rows)
-{
-    auto fn = tc::encode_fn();
-    if (!fn) return false;
-    const size_t es = precision == 0 ? 8 : 4;
-    cuuint64_t dims[2] = {(cuuint64_t)inner, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)(inner * es)};
-    cuuint32_t box[2] = {(cuuint32_t)box_inner, (cuuint32_t)box_rows};
-    cuuint32_t estr[2] = {1, 1};
-    return fn(map, precision == 0 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
-              2, const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
-}
-
 int tc_kpitch(int N) { return (N + 63) / 64 * 64; }
 int tc_bn() { return tc::BN; }
 int tc_bm() { return tc::BM; }
@@ -339,15 +340,15 @@ cudaError_t launch_split_bf16(const float *x, int rows, int N, int kp, void *hi,
 
 cudaError_t launch_list_proj_tc(const CUtensorMap &Ah, const CUtensorMap &Al, const CUtensorMap &Bh,
                                 const CUtensorMap &Bl, int M, int kp, int R, int nrec_chunk,
-                                int rec_begin, int n_rec_total, int Lq, void *series, int Q,
-                                int qoff, int *status, cudaStream_t st)
+                                int rec_begin, int n_rec_total, int Lq, const double *win,
+                                void *series, int nqb, int qoff, int *status, cudaStream_t st)
 {
     auto k = tc::list_proj_tc_kernel;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM);
     if (e != cudaSuccess) return e;
     dim3 grid((M + tc::BM - 1) / tc::BM, (2 * Lq + tc::BN - 1) / tc::BN);
     k<<<grid, 128, tc::SMEM, st>>>(Ah, Al, Bh, Bl, M, kp / tc::BK, R, nrec_chunk, rec_begin,
-                                   n_rec_total, Lq, (cplx<float> *)series, Q, qoff, status);
+                                   n_rec_total, Lq, win, (cplx<float> *)series, nqb, qoff, status);
     return cudaGetLastError();
 }
 

@@ -70,6 +70,21 @@ struct cplx {
     T x, y;
 };
 
+// Layout of a wave's windowed time series w[t] S(q,t): q in blocks of
+// QB = 16 / sizeof(cplx<T>) consecutive q (2 in FP32, 1 in FP64), each block
+// holding every record t of its q as [t][QB].  One block is a contiguous
+// run of n_rec * 16 bytes, so the time transform fetches whole sequences
+// with single bulk copies.  nqb = number of q blocks per (sample, component).
+template <typename T>
+__host__ __device__ constexpr int series_qb() { return 16 / (int)sizeof(cplx<T>); }
+
+template <typename T>
+__device__ __forceinline__ size_t series_off(int s, int c, int q, int t, int nqb, int n_rec)
+{
+    constexpr int QB = series_qb<T>();
+    return ((((size_t)s * 3 + c) * nqb + q / QB) * n_rec + t) * QB + q % QB;
+}
+
 __device__ __forceinline__ double warp_sum(double v)
 {
 #pragma unroll

@@ -16,26 +16,26 @@ cudaError_t launch_rk(const LatticeDev &L, const RKJob &J, int precision, bool g
 size_t grid_proj_smem(int G, int precision, const FFTPlan &p);
 cudaError_t launch_grid_proj(const void *snap, int precision, int N, int W, int R, int nrec_chunk,
                              int rec_begin, int n_rec_total, const int *grid_map,
-                             const FFTPlan &plan, const void *tw, double scale, void *series,
-                             int Q, cudaStream_t st);
+                             const FFTPlan &plan, const void *tw, double scale, const double *win,
+                             void *series, int nqb, cudaStream_t st);
 cudaError_t launch_list_proj_simt(const void *snap, int precision, int W, int R, int nrec_chunk,
                                   int N, int rec_begin, int n_rec_total, const void *P, int Lq,
-                                  void *series, int Q, int qoff, cudaStream_t st);
+                                  const double *win, void *series, int nqb, int qoff, cudaStream_t st);
+// q values per block of the series layout (series_qb) of a precision
+int series_qblock(int precision);
 int time_fft_qt(int n, int precision);
 size_t time_fft_smem(int n, int qt, int precision, const FFTPlan &p);
-int time_fft_box_rows(int n, int qt, int precision);
-cudaError_t launch_time_fft(const void *series, const CUtensorMap *smap, int precision, int W, int Q,
-                            int Qp, const FFTPlan &plan, const void *tw, const double *win,
-                            double *acc, int *status, cudaStream_t st);
+// whether the shared-memory time transform takes length n
+bool time_fft_fits(int n, int precision, const FFTPlan &p);
+cudaError_t launch_time_fft(const void *series, int precision, int W, int Q, int nqb,
+                            const FFTPlan &plan, const void *tw, double *acc, int *status,
+                            cudaStream_t st);
 cudaError_t launch_aos_to_soa(const double *in, double *out, int W, int N, cudaStream_t st);
 cudaError_t launch_soa_to_aos(const double *in, double *out, int W, int N, cudaStream_t st);
 cudaError_t launch_sum_rows(const double *rows, int W, int n, double *out, cudaStream_t st);
 
 // tensor-core list projection (proj_tc.cu)
 bool make_bf16_map(CUtensorMap *map, const void *base, int rows, int kp, int box_rows);
-// row-major [rows][inner] matrix of FP32 (precision 1) or FP64 (0) values
-bool make_real_map(CUtensorMap *map, const void *base, int precision, size_t inner, size_t rows,
-                   int box_inner, int box_rows);
 int tc_kpitch(int N);
 int tc_bn();
 int tc_bm();
@@ -43,7 +43,7 @@ cudaError_t launch_split_bf16(const float *x, int rows, int N, int kp, void *hi,
                               cudaStream_t st);
 cudaError_t launch_list_proj_tc(const CUtensorMap &Ah, const CUtensorMap &Al, const CUtensorMap &Bh,
                                 const CUtensorMap &Bl, int M, int kp, int R, int nrec_chunk,
-                                int rec_begin, int n_rec_total, int Lq, void *series, int Q,
-                                int qoff, int *status, cudaStream_t st);
+                                int rec_begin, int n_rec_total, int Lq, const double *win,
+                                void *series, int nqb, int qoff, int *status, cudaStream_t st);
 
 }  // namespace smd

@@ -95,6 +95,36 @@ def test_fp64_strided_grid_and_list_vs_oracle(ctx, oracle_mod, geom, L, J2, JX, 
     assert np.max(np.abs(r.qss - accq)) <= SPEC_TOL
 
 
+@pytest.mark.parametrize("precision", [_lib.SMD_FP64, _lib.SMD_FP32])
+@pytest.mark.parametrize("n_rec", [16, 32, 128, 512, 2048, 4096, 96, 1000])
+def test_time_transform_lengths_vs_oracle(ctx, oracle_mod, precision, n_rec):
+    """Every class of record count: powers of two 16 .. 4096 (register
+    radix-16 passes closing with radix 2, 4 or 8) and mixed radices (shared-
+    memory stages); an odd q count leaves the last q block half used."""
+    s = SMDSettings(geom="square", L=4, J2=0.6, dtm=0.002, ntm=n_rec, window="hann2")
+    lat, lid = _upload(ctx, s)
+    ql = np.random.default_rng(5).uniform(-np.pi, np.pi, size=(5, 2))
+    qid = ctx.qset(lid, use_grid=True, qlist=ql)
+    spins, _ = smp.make_samples(s, 2, "stripe", 0.4, 3)
+    win = smd.window("hann2", n_rec)
+    kw = dict(precision=precision, fix_every=16) if precision == _lib.SMD_FP32 else {}
+    r = ctx.run(lid, qid, spins, s.dtm, n_rec, win=win, **kw)
+    m = oracle_mod.Model(s, oracle_mod.make_lattice("square", 4))
+    acc = 0.0
+    for k in range(2):
+        acc = acc + oracle_mod.dyn_spectrum(m, spins[k], s.dtm, n_rec, win=win, qlist=ql,
+                                            pos=lat.grid_positions(),
+                                            list_scale=1.0 / lat.G)["spec"]
+    acc /= 2
+    if precision == _lib.SMD_FP64:
+        assert np.max(np.abs(r.spec - acc)) <= SPEC_TOL * np.max(np.abs(acc))
+    else:
+        G2 = lat.G * lat.G
+        for part in (slice(0, G2), slice(G2, None)):
+            a, b = r.spec[:, part], acc[:, part]
+            assert np.linalg.norm(a - b) / np.linalg.norm(b) <= 1e-3
+
+
 def test_list_points_on_the_grid_equal_grid_values(ctx):
     s = SMDSettings(geom="kagome", L=6, J2=0.3, dtm=0.01, ntm=16)
     lat, lid = _upload(ctx, s)
