@@ -1,300 +1,22 @@
-// fft_kernels.cu -- spatial projection S(q,t) and the windowed time
-// transform |S(q,w)|^2 accumulated over samples.
-//
-// Grid q (get_SqData_iMKL, Codes_Folder/subrouts.cpp:8330-8432): each record's
-// spins are embedded into the G x G DFT grid through gridMap (empty grid
-// points are zero), transformed by a forward 2D DFT (sign -1, unscaled) and
-// scaled by sqrt(1 / G^2).  One CTA transforms one (sample, record,
-// component) grid in shared memory: G row transforms, then G column
-// transforms, each a mixed-radix Stockham FFT (radices 4, 2, 3, 5, and any
-// other prime directly).
+// fft_kernels.cu -- list projection (FP64 form) and the time transform
+// |S(q,w)|^2 accumulated over samples.
 //
 // List q (get_qct_SqData, Codes_Folder/subrouts.cpp:8460-8525): S(q_l) =
 // scale sum_k S_k exp(-i q_l . pos_k), a dense contraction of the snapshot
-// rows with a phase table; the FP64 form runs it as a tiled SIMT GEMM.
+// rows with a phase table; the FP64 form runs it as a tiled SIMT GEMM (the
+// FP32 form on the tensor cores, proj_tc.cu).  The grid q are in
+// grid_proj.cu.
 //
-// Time transform (Codes_Folder/subrouts.cpp:12062-12109): x[t] = w[t] S(q,t),
-// forward FFT of length n_rec, |X|^2 / n_rec.  One CTA owns QT consecutive q
-// of one component, loops over every sample of the wave and keeps the sum
-// over samples in registers, so the accumulation needs no atomics and is
-// deterministic.
+// Time transform (Codes_Folder/subrouts.cpp:12062-12109): x[t] = w[t] S(q,t)
+// (the projections store the window-weighted series), forward FFT of length
+// n_rec, |X|^2 / n_rec.  A block owns consecutive q of one component, loops
+// over every sample of the wave and keeps the sum over samples in
+// registers, so the accumulation needs no atomics and is deterministic.
 #include <cuda.h>
 
-#include "smd_device.cuh"
+#include "fft_device.cuh"
 
 namespace smd {
-
-template <typename T>
-__device__ __forceinline__ cplx<T> cmul(cplx<T> a, cplx<T> b)
-{
-    return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
-}
-
-template <typename T>
-__device__ __forceinline__ cplx<T> cadd(cplx<T> a, cplx<T> b) { return {a.x + b.x, a.y + b.y}; }
-
-template <typename T>
-__device__ __forceinline__ cplx<T> csub(cplx<T> a, cplx<T> b) { return {a.x - b.x, a.y - b.y}; }
-
-// Radix-4 DFT (sign -1) of (a, b, c, d) in place: X0..X3 in a..d.
-template <typename T>
-__device__ __forceinline__ void dft4(cplx<T> &a, cplx<T> &b, cplx<T> &c, cplx<T> &d)
-{
-    const cplx<T> s0 = cadd(a, c), s1 = csub(a, c), s2 = cadd(b, d), s3 = csub(b, d);
-    // -i * s3 = (s3.y, -s3.x)
-    a = cadd(s0, s2);
-    c = csub(s0, s2);
-    b = {s1.x + s3.y, s1.y - s3.x};
-    d = {s1.x - s3.y, s1.y + s3.x};
-}
-
-// In-register forward DFT of radix R (sign -1).  For R outside
-// {2, 3, 4, 8, 16} the twiddle table of the full length n
-// (tw[j] = exp(-2 pi i j / n)) gives the R-th roots.
-template <typename T, int R>
-__device__ __forceinline__ void dft_small(cplx<T> (&v)[R], const cplx<T> *tw, int n)
-{
-    if constexpr (R == 2) {
-        cplx<T> a = v[0], b = v[1];
-        v[0] = cadd(a, b);
-        v[1] = csub(a, b);
-    } else if constexpr (R == 4) {
-        cplx<T> a = v[0], b = v[1], c = v[2], d = v[3];
-        cplx<T> s0 = cadd(a, c), s1 = csub(a, c), s2 = cadd(b, d), s3 = csub(b, d);
-        // -i * s3 = (s3.y, -s3.x)
-        v[0] = cadd(s0, s2);
-        v[2] = csub(s0, s2);
-        v[1] = {s1.x + s3.y, s1.y - s3.x};
-        v[3] = {s1.x - s3.y, s1.y + s3.x};
-    } else if constexpr (R == 3) {
-        const T h = T(0.86602540378443864676);   // sqrt(3)/2
-        cplx<T> a = v[0], b = v[1], c = v[2];
-        cplx<T> s = cadd(b, c), d = csub(b, c);
-        cplx<T> m = {a.x - T(0.5) * s.x, a.y - T(0.5) * s.y};
-        // -i h d = (h d.y, -h d.x)
-        v[0] = cadd(a, s);
-        v[1] = {m.x + h * d.y, m.y - h * d.x};
-        v[2] = {m.x - h * d.y, m.y + h * d.x};
-    } else if constexpr (R == 8) {
-        // 8 = 2 x 4: radix-4 over r1 (r = r0 + 2 r1), twiddle w8^(r0 p0),
-        // radix-2 over r0; X[p0 + 4 p1] lands in v[2 p0 + p1]
-        const T h = T(0.70710678118654752440);   // sqrt(1/2)
-#pragma unroll
-        for (int r0 = 0; r0 < 2; r0++) dft4(v[r0], v[r0 + 2], v[r0 + 4], v[r0 + 6]);
-        v[3] = {h * (v[3].x + v[3].y), h * (v[3].y - v[3].x)};    // w8^1
-        v[5] = {v[5].y, -v[5].x};                                 // w8^2 = -i
-        v[7] = {h * (v[7].y - v[7].x), -h * (v[7].x + v[7].y)};   // w8^3
-        cplx<T> u[8];
-#pragma unroll
-        for (int p0 = 0; p0 < 4; p0++) {
-            u[p0] = cadd(v[2 * p0], v[2 * p0 + 1]);
-            u[p0 + 4] = csub(v[2 * p0], v[2 * p0 + 1]);
-        }
-#pragma unroll
-        for (int p = 0; p < 8; p++) v[p] = u[p];
-    } else if constexpr (R == 16) {
-        // 16 = 4 x 4: radix-4 over r1 (r = r0 + 4 r1), twiddle w16^(r0 p0),
-        // radix-4 over r0; X[p0 + 4 p1] lands in v[4 p0 + p1]
-        const T h = T(0.70710678118654752440);    // sqrt(1/2)
-        const T c1 = T(0.92387953251128675613);   // cos(pi/8)
-        const T s1 = T(0.38268343236508977173);   // sin(pi/8)
-#pragma unroll
-        for (int r0 = 0; r0 < 4; r0++) dft4(v[r0], v[r0 + 4], v[r0 + 8], v[r0 + 12]);
-        // y[r0][p0] sits in v[r0 + 4 p0]
-        v[5] = cmul(v[5], cplx<T>{c1, -s1});                          // w16^1
-        v[9] = {h * (v[9].x + v[9].y), h * (v[9].y - v[9].x)};        // w16^2
-        v[13] = cmul(v[13], cplx<T>{s1, -c1});                        // w16^3
-        v[6] = {h * (v[6].x + v[6].y), h * (v[6].y - v[6].x)};        // w16^2
-        v[10] = {v[10].y, -v[10].x};                                  // w16^4 = -i
-        v[14] = {h * (v[14].y - v[14].x), -h * (v[14].x + v[14].y)};  // w16^6
-        v[7] = cmul(v[7], cplx<T>{s1, -c1});                          // w16^3
-        v[11] = {h * (v[11].y - v[11].x), -h * (v[11].x + v[11].y)};  // w16^6
-        v[15] = cmul(v[15], cplx<T>{-c1, s1});                        // w16^9
-#pragma unroll
-        for (int p0 = 0; p0 < 4; p0++) dft4(v[4 * p0], v[4 * p0 + 1], v[4 * p0 + 2], v[4 * p0 + 3]);
-        // v[4 p0 + p1] = X[p0 + 4 p1]; reorder to natural order
-        cplx<T> u[16];
-#pragma unroll
-        for (int p0 = 0; p0 < 4; p0++)
-#pragma unroll
-            for (int p1 = 0; p1 < 4; p1++) u[p0 + 4 * p1] = v[4 * p0 + p1];
-#pragma unroll
-        for (int p = 0; p < 16; p++) v[p] = u[p];
-    } else {
-        cplx<T> u[R];
-#pragma unroll
-        for (int p = 0; p < R; p++) {
-            cplx<T> s = v[0];
-#pragma unroll
-            for (int q = 1; q < R; q++) {
-                const cplx<T> w = tw[((q * p) % R) * (n / R)];
-                s = cadd(s, cmul(v[q], w));
-            }
-            u[p] = s;
-        }
-#pragma unroll
-        for (int p = 0; p < R; p++) v[p] = u[p];
-    }
-}
-
-// One Stockham stage of radix R over nseq sequences of length n held in
-// shared memory: element x of sequence q sits at buf[q * ss + x * es].
-// Every thread first loads all of its butterflies, then (after a barrier)
-// writes them, so the stage runs in place.  NB = butterflies per thread.
-template <typename T, int R, int NB>
-__device__ __forceinline__ void stockham_stage(cplx<T> *buf, int n, int nseq, int ss, int es,
-                                               int Ns, const cplx<T> *tw)
-{
-    const int m = n / R, nb = nseq * m;
-    // Consecutive threads take consecutive elements: along a sequence when
-    // its elements are adjacent (es == 1), across sequences otherwise, so
-    // shared-memory accesses stay free of bank conflicts.
-    const bool qfast = es != 1;
-    cplx<T> v[NB][R];
-#pragma unroll
-    for (int u = 0; u < NB; u++) {
-        const int b = threadIdx.x + u * blockDim.x;
-        if (b < nb) {
-            const int q = qfast ? b % nseq : b / m;
-            const int j = qfast ? b / nseq : b - q * m;
-#pragma unroll
-            for (int r = 0; r < R; r++) v[u][r] = buf[q * ss + (j + r * m) * es];
-        }
-    }
-    __syncthreads();
-    const int tstep = n / (Ns * R);
-#pragma unroll
-    for (int u = 0; u < NB; u++) {
-        const int b = threadIdx.x + u * blockDim.x;
-        if (b < nb) {
-            const int q = qfast ? b % nseq : b / m;
-            const int j = qfast ? b / nseq : b - q * m;
-            const int k = j % Ns;
-#pragma unroll
-            for (int r = 1; r < R; r++) v[u][r] = cmul(v[u][r], tw[(r * k) * tstep]);   // index < n
-            dft_small<T, R>(v[u], tw, n);
-            const int idx = (j / Ns) * Ns * R + k;
-#pragma unroll
-            for (int r = 0; r < R; r++) buf[q * ss + (idx + r * Ns) * es] = v[u][r];
-        }
-    }
-    __syncthreads();
-}
-
-// Any other radix: one butterfly at a time, streaming from a copy of the
-// sequences.  Kept out of line so that its register needs stay apart from
-// the radix-4 / radix-2 path; thread mapping as in stockham_stage.
-template <typename T>
-__device__ __noinline__ void stockham_stage_generic(cplx<T> *buf, int n, int nseq, int ss, int es,
-                                                    int Ns, int R, const cplx<T> *tw,
-                                                    cplx<T> *scratch)
-{
-    // scratch: a copy of the sequences (same layout), so loads and stores
-    // touch different arrays
-    const bool qfast = es != 1;
-    const int total = nseq * n;
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
-        const int q = qfast ? e % nseq : e / n;
-        const int x = qfast ? e / nseq : e - q * n;
-        scratch[q * ss + x * es] = buf[q * ss + x * es];
-    }
-    __syncthreads();
-    const int m = n / R, nb = nseq * m, tstep = n / (Ns * R);
-    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-        const int q = qfast ? b % nseq : b / m;
-        const int j = qfast ? b / nseq : b - q * m;
-        const int k = j % Ns;
-        const int idx = (j / Ns) * Ns * R + k;
-        for (int p = 0; p < R; p++) {
-            cplx<T> s = {T(0), T(0)};
-            for (int r = 0; r < R; r++) {
-                cplx<T> x = scratch[q * ss + (j + r * m) * es];
-                if (r) x = cmul(x, tw[(r * k) * tstep]);   // index < n
-                s = cadd(s, cmul(x, tw[((r * p) % R) * (n / R)]));
-            }
-            buf[q * ss + (idx + p * Ns) * es] = s;
-        }
-    }
-    __syncthreads();
-}
-
-// Full transform.  C = values each thread holds in registers during a
-// stage (8 keeps a 1024-thread CTA within 64 registers per thread; 16 only
-// for the largest grids).  Radices come from the host plan (product = n);
-// every stage needs nseq * n <= C * blockDim.x.  KIND selects the stages a
-// kernel is built with, so that each plan pays only for the stages it uses:
-//   KIND 0: radix 4 and 2 inline (plans of radices 2 and 4);
-//   KIND 1: radix 4, 2 and 3 inline (plans of radices 2, 3 and 4);
-//   KIND 2: radix 4 and 2 inline, any other radix through the out-of-line
-//           streaming stage, whose register needs stay apart from the rest.
-template <typename T, int C, int KIND>
-__device__ void smem_fft(cplx<T> *buf, int n, int nseq, int ss, int es, const int *radix,
-                         int nst, const cplx<T> *tw, cplx<T> *scratch)
-{
-    int Ns = 1;
-    for (int s = 0; s < nst; s++) {
-        const int R = radix[s];
-        switch (R) {
-        case 4: stockham_stage<T, 4, (C + 3) / 4>(buf, n, nseq, ss, es, Ns, tw); break;
-        case 2: stockham_stage<T, 2, (C + 1) / 2>(buf, n, nseq, ss, es, Ns, tw); break;
-        default:
-            if (KIND == 1) stockham_stage<T, 3, (C + 2) / 3>(buf, n, nseq, ss, es, Ns, tw);
-            if (KIND == 2) stockham_stage_generic<T>(buf, n, nseq, ss, es, Ns, R, tw, scratch);
-            break;
-        }
-        Ns *= R;
-    }
-}
-
-// ---------------------------------------------------------- grid projection
-
-// grid 2D FFT of snapshot rows; blockIdx.x = (s * R + slot) * 3 + c.
-// C = 8 serves grids up to 64 x 64 with at most 512 threads (128 registers
-// each); C = 16 the larger ones with up to 1024 threads.
-template <typename TS, typename T, int C, int KIND>
-__global__ void __launch_bounds__(C <= 8 ? 512 : 1024) grid_proj_kernel(
-    const TS *__restrict__ snap, int N, int R, int rec_begin, int n_rec_total,
-    const int *__restrict__ grid_map, FFTPlan plan, const cplx<T> *__restrict__ tw_g,
-    double scale, const double *__restrict__ win, cplx<T> *__restrict__ series, int nqb,
-    int use_scratch)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int G = plan.n, GG = G * G;
-    cplx<T> *buf = reinterpret_cast<cplx<T> *>(smem_raw);
-    cplx<T> *tw = buf + GG;
-    cplx<T> *scratch = use_scratch ? tw + G : nullptr;
-    const int row = blockIdx.x, s = blockIdx.y;
-    const int c = row % 3, slot = row / 3;
-    const TS *x = snap + ((size_t)s * R * 3 + row) * N;
-    for (int k = threadIdx.x; k < G; k += blockDim.x) tw[k] = tw_g[k];
-    for (int k = threadIdx.x; k < GG; k += blockDim.x) {
-        const int idx = grid_map[k];
-        buf[k] = {idx < 0 ? T(0) : T(x[idx]), T(0)};
-    }
-    __syncthreads();
-    smem_fft<T, C, KIND>(buf, G, G, G, 1, plan.radix, plan.nst, tw, scratch);   // rows
-    smem_fft<T, C, KIND>(buf, G, G, 1, G, plan.radix, plan.nst, tw, scratch);   // columns
-    // windowed output, q = k: one 16-byte store per q block
-    const int t = rec_begin + slot;
-    constexpr int QB = series_qb<T>();
-    cplx<T> *out = series + series_off<T>(s, c, 0, t, nqb, n_rec_total);
-    const size_t bstride = (size_t)n_rec_total * QB;
-    const T sc = T(scale * win[t]);
-    for (int b = threadIdx.x; b < GG / QB; b += blockDim.x) {
-        cplx<T> v[QB];
-#pragma unroll
-        for (int i = 0; i < QB; i++) v[i] = {sc * buf[b * QB + i].x, sc * buf[b * QB + i].y};
-        if constexpr (QB == 2)
-            *reinterpret_cast<float4 *>(out + b * bstride) =
-                make_float4((float)v[0].x, (float)v[0].y, (float)v[QB - 1].x, (float)v[QB - 1].y);
-        else
-            *reinterpret_cast<double2 *>(out + b * bstride) = make_double2((double)v[0].x, (double)v[0].y);
-    }
-    if (GG % QB && threadIdx.x == 0) {   // a half block shared with the first list q
-        const int k = GG - 1;
-        out[(k / QB) * bstride + k % QB] = {sc * buf[k].x, sc * buf[k].y};
-    }
-}
 
 // ---------------------------------------------------------- list projection
 
@@ -365,7 +87,7 @@ __global__ void __launch_bounds__(256) list_proj_simt_kernel(
 // Generic lengths.  blockIdx.x = c * ntile + q-tile of QT sequences (QT a
 // multiple of the q block).  The series is already windowed.  Sums over the
 // W samples of the wave into acc[c][q][n_rec] (added to what acc holds).
-template <typename T, int KIND>
+template <typename T, int FL>
 __global__ void __launch_bounds__(1024) time_fft_kernel(
     const cplx<T> *__restrict__ series, int W, int Q, int nqb, int QT, FFTPlan plan,
     const cplx<T> *__restrict__ tw_g, double *__restrict__ acc, int use_scratch)
@@ -392,7 +114,7 @@ __global__ void __launch_bounds__(1024) time_fft_kernel(
             buf[(b * QB + qi) * n + t] = src[e];
         }
         __syncthreads();
-        smem_fft<T, MAXA, KIND>(buf, n, QT, n, 1, plan.radix, plan.nst, tw_g, scratch);
+        smem_fft<T, MAXA, FL>(buf, n, QT, n, 1, plan.radix, plan.nst, tw_g, scratch);
 #pragma unroll
         for (int u = 0; u < MAXA; u++) {
             const int e = threadIdx.x + u * blockDim.x;
@@ -724,73 +446,16 @@ __global__ void sum_rows_kernel(const double *__restrict__ rows, int W, int n,
 
 // ---------------------------------------------------------- launchers
 
-static int fft_threads(int elems, int cap)
+// time kernel instance of a stage set (plans of make_plan carry no radix 16 or 8)
+template <typename T>
+static auto time_kernel(int fl)
 {
-    int t = (elems + cap - 1) / cap;
-    t = (t + 31) / 32 * 32;
-    if (t < 128) t = 128;
-    if (t > 1024) t = 1024;
-    return t;
-}
-
-// Stage set a plan needs (the KIND of smem_fft); kind 2 runs a stage through
-// the streaming stage, which needs a scratch copy of the sequences.
-static int plan_kind(const FFTPlan &p)
-{
-    int kind = 0;
-    for (int s = 0; s < p.nst; s++) {
-        if (p.radix[s] == 3) kind = kind < 1 ? 1 : kind;
-        else if (p.radix[s] != 2 && p.radix[s] != 4) kind = 2;
+    switch (fl & (FK_R3 | FK_GEN)) {
+    case 0: return time_fft_kernel<T, 0>;
+    case FK_R3: return time_fft_kernel<T, FK_R3>;
+    case FK_GEN: return time_fft_kernel<T, FK_GEN>;
+    default: return time_fft_kernel<T, FK_R3 | FK_GEN>;
     }
-    return kind;
-}
-
-static bool plan_generic(const FFTPlan &p) { return plan_kind(p) == 2; }
-
-// kernel instance of a stage set
-template <typename F0, typename F1, typename F2>
-static auto by_kind(int kind, F0 k0, F1 k1, F2 k2) { return kind == 0 ? k0 : kind == 1 ? k1 : k2; }
-
-size_t grid_proj_smem(int G, int precision, const FFTPlan &p)
-{
-    const size_t e = precision == 0 ? sizeof(cplx<double>) : sizeof(cplx<float>);
-    size_t b = ((size_t)G * G + G) * e;
-    if (plan_generic(p)) b += (size_t)G * G * e;
-    return b;
-}
-
-cudaError_t launch_grid_proj(const void *snap, int precision, int N, int W, int R, int nrec_chunk,
-                             int rec_begin, int n_rec_total, const int *grid_map, const FFTPlan &plan,
-                             const void *tw, double scale, const double *win, void *series, int nqb,
-                             cudaStream_t st)
-{
-    const int G = plan.n;
-    const size_t smem = grid_proj_smem(G, precision, plan);
-    const bool big = G * G > 4096;   // grids up to 128 x 128 hold 16 values per thread
-    const int threads = fft_threads(G * G, big ? 16 : 8);
-    const int kind = plan_kind(plan), gen = kind == 2 ? 1 : 0;
-    // only the first nrec_chunk slots of each sample hold records
-    dim3 grid(nrec_chunk * 3, W);
-    if (precision == 0) {
-        auto k = big ? by_kind(kind, grid_proj_kernel<double, double, 16, 0>,
-                               grid_proj_kernel<double, double, 16, 1>, grid_proj_kernel<double, double, 16, 2>)
-                     : by_kind(kind, grid_proj_kernel<double, double, 8, 0>,
-                               grid_proj_kernel<double, double, 8, 1>, grid_proj_kernel<double, double, 8, 2>);
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k<<<grid, threads, smem, st>>>((const double *)snap, N, R, rec_begin, n_rec_total,
-                                       grid_map, plan, (const cplx<double> *)tw, scale, win,
-                                       (cplx<double> *)series, nqb, gen);
-    } else {
-        auto k = big ? by_kind(kind, grid_proj_kernel<float, float, 16, 0>, grid_proj_kernel<float, float, 16, 1>,
-                               grid_proj_kernel<float, float, 16, 2>)
-                     : by_kind(kind, grid_proj_kernel<float, float, 8, 0>, grid_proj_kernel<float, float, 8, 1>,
-                               grid_proj_kernel<float, float, 8, 2>);
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k<<<grid, threads, smem, st>>>((const float *)snap, N, R, rec_begin, n_rec_total,
-                                       grid_map, plan, (const cplx<float> *)tw, scale, win,
-                                       (cplx<float> *)series, nqb, gen);
-    }
-    return cudaGetLastError();
 }
 
 cudaError_t launch_list_proj_simt(const void *snap, int precision, int W, int R, int nrec_chunk,
@@ -897,14 +562,14 @@ cudaError_t launch_time_fft(const void *series, int precision, int W, int Q, int
     const size_t smem = time_fft_smem(n, qt, precision, plan);
     const int threads = fft_threads(qt * n, 8);
     const int ntile = (nqb * qb + qt - 1) / qt;
-    const int kind = plan_kind(plan), gen = kind == 2 ? 1 : 0;
+    const int fl = fft_plan_flags(plan), gen = (fl & FK_GEN) ? 1 : 0;
     if (precision == 0) {
-        auto k = by_kind(kind, time_fft_kernel<double, 0>, time_fft_kernel<double, 1>, time_fft_kernel<double, 2>);
+        auto k = time_kernel<double>(fl);
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k<<<3 * ntile, threads, smem, st>>>((const cplx<double> *)series, W, Q, nqb, qt, plan,
                                             (const cplx<double> *)tw, acc, gen);
     } else {
-        auto k = by_kind(kind, time_fft_kernel<float, 0>, time_fft_kernel<float, 1>, time_fft_kernel<float, 2>);
+        auto k = time_kernel<float>(fl);
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k<<<3 * ntile, threads, smem, st>>>((const cplx<float> *)series, W, Q, nqb, qt, plan,
                                             (const cplx<float> *)tw, acc, gen);

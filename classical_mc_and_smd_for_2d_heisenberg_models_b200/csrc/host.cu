@@ -149,11 +149,18 @@ int cuda_fail(smd_ctx *c, cudaError_t e, const char *where)
         if (_e != cudaSuccess) return cuda_fail(ctx, _e, where); \
     } while (0)
 
-bool make_plan(int n, FFTPlan &p)
+// Radices of an FFT of length n.  wide: radix 16 and 8 first (the grid
+// transform, whose stages hold 16 values per thread), else radix 4 first.
+bool make_plan(int n, FFTPlan &p, bool wide)
 {
     p.n = n;
     p.nst = 0;
     int m = n;
+    if (wide) {
+        for (int r : {16, 8}) {
+            while (m % r == 0 && p.nst < 16) { p.radix[p.nst++] = r; m /= r; }
+        }
+    }
     while (m % 4 == 0 && m > 4 && p.nst < 16) { p.radix[p.nst++] = 4; m /= 4; }
     for (int r : {4, 2, 3, 5}) {
         while (m % r == 0 && m > 1 && p.nst < 16) { p.radix[p.nst++] = r; m /= r; }
@@ -447,10 +454,10 @@ extern "C" int smd_qset_upload(smd_ctx *ctx, int lattice_id, int use_grid, int n
     Q->list_scale = list_scale;
     if (Q->Q <= 0) return fail(ctx, SMD_EINVAL, "qset: empty");
     if (use_grid) {
-        if (!make_plan(L.G, Q->gplan)) return fail(ctx, SMD_EINVAL, "qset: grid size has a prime factor > 64");
+        if (!make_plan(L.G, Q->gplan, true)) return fail(ctx, SMD_EINVAL, "qset: grid size has a prime factor > 64");
         if ((size_t)L.G * L.G > 16384) return fail(ctx, SMD_EINVAL, "qset: grid larger than 128 x 128");
-        if ((size_t)L.G * L.G > 8192 || grid_proj_smem(L.G, 0, Q->gplan) > 200 * 1024)
-            Q->fp64_ok = 0;
+        if (!grid_proj_ng(L.G, 1, Q->gplan)) return fail(ctx, SMD_EINVAL, "qset: grid too large for the shared-memory transform");
+        if (!grid_proj_ng(L.G, 0, Q->gplan)) Q->fp64_ok = 0;
         CK(upload_twiddles(L.G, Q->tw64, Q->tw32), "twiddles");
     }
     if (n_list > 0) {
@@ -709,7 +716,7 @@ int prepare(smd_ctx *ctx, const smd_job_desc *job, JobGeom &g)
     auto pi = ctx->tplans.find(g.n_rec);
     if (pi == ctx->tplans.end()) {
         auto P = std::make_unique<Plan>();
-        if (!make_plan(g.n_rec, P->p)) return fail(ctx, SMD_EINVAL, "job: n_rec has a prime factor > 64");
+        if (!make_plan(g.n_rec, P->p, false)) return fail(ctx, SMD_EINVAL, "job: n_rec has a prime factor > 64");
         CK(upload_twiddles(g.n_rec, P->tw64, P->tw32), "twiddles");
         pi = ctx->tplans.emplace(g.n_rec, std::move(P)).first;
     }

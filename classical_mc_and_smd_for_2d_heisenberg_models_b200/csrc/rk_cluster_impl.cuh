@@ -46,13 +46,14 @@ __device__ __forceinline__ float cl_coef(const ClusterParams &P, int e, int c, f
     return P.coef32[e][c];
 }
 
-// Register budget per own site: FP32 form 16 registers (FP64 spin, FP32
-// copy, stage input, accumulator, mask), FP64 form 19.
+// Block sizes per sites-per-thread: each own site keeps in registers its
+// FP64 spin, the FP32 copy (FP32 form), stage input, accumulator, mask, up
+// to six packed neighbour words and two push codes, so a thread of SPT
+// sites needs about 40 SPT + 20 registers.
 template <typename T>
 __host__ __device__ constexpr int cl_maxt(int spt)
 {
-    return sizeof(T) == 4 ? (spt <= 1 ? 1024 : spt <= 2 ? 768 : 512)
-                          : (spt <= 1 ? 1024 : spt <= 2 ? 768 : 512);
+    return spt <= 1 ? 768 : spt <= 2 ? 576 : 512;
 }
 
 template <typename T, int SPT, int ZT>
@@ -112,6 +113,27 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
     }
     int slot = 0;
     const double hz = P.h;
+    // FP32 copy of the master spins (FP32 form): stage inputs need no
+    // conversion from FP64 at every stage
+    constexpr bool SF = sizeof(T) == 4;
+    T Sf[SF ? SPT : 1][3];
+    auto spin = [&](int k, int c) -> T {
+        if constexpr (SF) return Sf[k][c];
+        else return S[k][c];
+    };
+    auto sync_spin = [&](int k) {
+        if constexpr (SF)
+#pragma unroll
+            for (int c = 0; c < 3; c++) Sf[k][c] = T(S[k][c]);
+    };
+#pragma unroll
+    for (int k = 0; k < SPT; k++) sync_spin(k);
+    // packed neighbour words and the first two push codes of each own site
+    // live in registers (after the table load below); further push codes
+    // stay in shared memory
+    constexpr bool NBREG = SPT * (ZT / 2) <= 12;
+    uint32_t nbw[NBREG ? SPT : 1][NBREG ? ZT / 2 : 1];
+    int pc0[SPT], pc1[SPT];
 
     // ---- helpers
     auto cl_sync = [&]() { cl.sync(); };
@@ -145,14 +167,18 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
         slot ^= 1;
     };
 
-    // local store of an own site's value plus the pushes into halo copies
-    auto put = [&](Vec4<T> *buf, int li, const Vec4<T> &v) {
+    // local store of own site k's value plus the pushes into halo copies
+    // (push codes fill from slot 0, so pc0 < 0 means no pushes at all)
+    auto put = [&](Vec4<T> *buf, int k, int li, const Vec4<T> &v) {
         buf[li] = v;
-        for (int p = 0; p < P.pmax; p++) {
-            const int code = push[p * nom + li];
-            if (code >= 0) {
-                Vec4<T> *rb = cl.map_shared_rank(buf, code >> 16);
-                rb[code & 0xffff] = v;
+        if (pc0[k] >= 0) {
+            cl.map_shared_rank(buf, pc0[k] >> 16)[pc0[k] & 0xffff] = v;
+            if (pc1[k] >= 0) {
+                cl.map_shared_rank(buf, pc1[k] >> 16)[pc1[k] & 0xffff] = v;
+                for (int p = 2; p < P.pmax; p++) {
+                    const int code = push[p * nom + li];
+                    if (code >= 0) cl.map_shared_rank(buf, code >> 16)[code & 0xffff] = v;
+                }
             }
         }
     };
@@ -167,13 +193,19 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
             }
         }
     };
+    // packed neighbour word j of own site k (local index li)
+    auto nbword = [&](int k, int li, int j) -> uint32_t {
+        if constexpr (NBREG) return nbw[k][j];
+        else return idx[j * nom + li];
+    };
 
-    // field of own site li from buffer src (mask_i applied, -h z added)
-    auto field = [&](const Vec4<T> *src, int li, T m, T h[3]) {
+    // field of own site k (local index li) from buffer src (mask applied,
+    // -h z added)
+    auto field = [&](const Vec4<T> *src, int k, int li, T m, T h[3]) {
         T s0 = zero, s1 = zero, s2 = zero;
 #pragma unroll
         for (int e = 0; e < ZT; e += 2) {
-            const uint32_t w = idx[(e >> 1) * nom + li];
+            const uint32_t w = nbword(k, li, e >> 1);
             const Vec4<T> a = src[w & 0xffffu];
             const Vec4<T> b = src[w >> 16];
             s0 = fma(cl_coef(P, e, 0, zero), a.x, s0);
@@ -187,11 +219,11 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
         h[1] = m * s1;
         h[2] = m * s2 - T(hz);
     };
-    auto field64 = [&](int li, double m, double h[3]) {
+    auto field64 = [&](int k, int li, double m, double h[3]) {
         double s0 = 0.0, s1 = 0.0, s2 = 0.0;
 #pragma unroll
         for (int e = 0; e < ZT; e += 2) {
-            const uint32_t w = idx[(e >> 1) * nom + li];
+            const uint32_t w = nbword(k, li, e >> 1);
             const int a = w & 0xffffu, b = w >> 16;
             s0 = fma(P.coef64[e][0], D[a], s0);
             s1 = fma(P.coef64[e][1], D[Np + a], s1);
@@ -250,10 +282,10 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
                 double h[3];
                 if (sizeof(T) == 8) {
                     T ht[3];
-                    field(A, li, mk[k], ht);
+                    field(A, k, li, mk[k], ht);
                     h[0] = ht[0]; h[1] = ht[1]; h[2] = ht[2];
                 } else {
-                    field64(li, (double)mk[k], h);
+                    field64(k, li, (double)mk[k], h);
                 }
                 e += S[k][0] * h[0] + S[k][1] * h[1] + S[k][2] * h[2] - hz * S[k][2];
             }
@@ -281,7 +313,7 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
             const int li = tid + k * NT;
             if (li < n_own) {
                 const T m = mk[k];
-                put(A, li, {m * T(S[k][0]), m * T(S[k][1]), m * T(S[k][2]), zero});
+                put(A, k, li, {m * spin(k, 0), m * spin(k, 1), m * spin(k, 2), zero});
             }
         }
         if (tid == 0) {
@@ -313,6 +345,16 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
     };
 
     cl_sync();   // every CTA of the cluster is running before any remote access
+#pragma unroll
+    for (int k = 0; k < SPT; k++) {
+        const int li = tid + k * NT;
+        const bool own = li < n_own;
+        if constexpr (NBREG)
+#pragma unroll
+            for (int j = 0; j < ZT / 2; j++) nbw[k][j] = own ? idx[j * nom + li] : 0u;
+        pc0[k] = (own && P.pmax > 0) ? push[li] : -1;
+        pc1[k] = (own && P.pmax > 1) ? push[nom + li] : -1;
+    }
 
     double E0, drift = 0.0;
     if (J.rec_begin == 0) {
@@ -349,10 +391,10 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
                 const int li = tid + k * NT;
                 if (li < n_own) {
                     T h[3], Sp[3], Pv[3];
-                    field(A, li, mk[k], h);
-                    Sp[0] = T(S[k][0]);
-                    Sp[1] = T(S[k][1]);
-                    Sp[2] = T(S[k][2]);
+                    field(A, k, li, mk[k], h);
+                    Sp[0] = spin(k, 0);
+                    Sp[1] = spin(k, 1);
+                    Sp[2] = spin(k, 2);
                     if (sizeof(T) == 8 && per_step)
                         eref += S[k][0] * h[0] + S[k][1] * h[1] + S[k][2] * h[2] - hz * S[k][2];
                     Pv[0] = h[1] * Sp[2] - h[2] * Sp[1];
@@ -365,7 +407,7 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
                         Pin[k][c] = Sp[c] + T(0.5) * K;
                     }
                     const T m = mk[k];
-                    put(B, li, {m * Pin[k][0], m * Pin[k][1], m * Pin[k][2], zero});
+                    put(B, k, li, {m * Pin[k][0], m * Pin[k][1], m * Pin[k][2], zero});
                 }
             }
             cl_sync();
@@ -380,7 +422,7 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
                     const int li = tid + k * NT;
                     if (li < n_own) {
                         T h[3], Pv[3];
-                        field(src, li, mk[k], h);
+                        field(src, k, li, mk[k], h);
                         const T *Sp = Pin[k];
                         Pv[0] = h[1] * Sp[2] - h[2] * Sp[1];
                         Pv[1] = h[2] * Sp[0] - h[0] * Sp[2];
@@ -390,12 +432,12 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
                         for (int c = 0; c < 3; c++) {
                             const T K = dt * Pv[c];
                             acc[k][c] += f2 * K;
-                            nx[c] = T(S[k][c]) + cst * K;
+                            nx[c] = spin(k, c) + cst * K;
                         }
 #pragma unroll
                         for (int c = 0; c < 3; c++) Pin[k][c] = nx[c];
                         const T m = mk[k];
-                        put(dst, li, {m * nx[0], m * nx[1], m * nx[2], zero});
+                        put(dst, k, li, {m * nx[0], m * nx[1], m * nx[2], zero});
                     }
                 }
                 cl_sync();
@@ -406,7 +448,7 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
                 const int li = tid + k * NT;
                 if (li < n_own) {
                     T h[3], Pv[3];
-                    field(B, li, mk[k], h);
+                    field(B, k, li, mk[k], h);
                     const T *Sp = Pin[k];
                     Pv[0] = h[1] * Sp[2] - h[2] * Sp[1];
                     Pv[1] = h[2] * Sp[0] - h[0] * Sp[2];
@@ -420,6 +462,7 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
                     normalise(v);
 #pragma unroll
                     for (int c = 0; c < 3; c++) S[k][c] = v[c];
+                    sync_spin(k);
                 }
             }
             if (!fix) {
@@ -443,10 +486,10 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
                     double h[3], Pv[3];
                     if (sizeof(T) == 8) {
                         T ht[3];
-                        field(A, li, mk[k], ht);
+                        field(A, k, li, mk[k], ht);
                         h[0] = ht[0]; h[1] = ht[1]; h[2] = ht[2];
                     } else {
-                        field64(li, (double)mk[k], h);
+                        field64(k, li, (double)mk[k], h);
                     }
                     Pv[0] = h[1] * S[k][2] - h[2] * S[k][1];
                     Pv[1] = h[2] * S[k][0] - h[0] * S[k][2];
@@ -482,6 +525,7 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
                     normalise(v);
 #pragma unroll
                     for (int c = 0; c < 3; c++) S[k][c] = v[c];
+                    sync_spin(k);
                 }
             }
             publishA();   // the reduction's cluster barrier ordered every read of A / D before this

@@ -13,6 +13,9 @@ int rk_max_sites(int precision);
 cudaError_t launch_rk(const LatticeDev &L, const RKJob &J, int precision, bool gen,
                       cudaStream_t st);
 
+// components per block of the grid transform (3 or 1); 0 when the grid
+// does not fit one block
+int grid_proj_ng(int G, int precision, const FFTPlan &p);
 size_t grid_proj_smem(int G, int precision, const FFTPlan &p);
 cudaError_t launch_grid_proj(const void *snap, int precision, int N, int W, int R, int nrec_chunk,
                              int rec_begin, int n_rec_total, const int *grid_map,
