@@ -141,34 +141,41 @@ __global__ void __launch_bounds__(1024) time_fft_kernel(
 // tile S that one bulk copy filled ([block][t][QB], as in the series) and
 // writes the work buffer Wb; each later pass reads and writes Wb in place;
 // the last keeps its outputs X[j + r n/R] in registers and adds |X|^2 / n to
-// the thread's accumulators.  Wb holds sequence qq at Wb[qq * PS + phys(i)]
-// with phys(i) = i + QB * (i / 16): the first pass writes 16 consecutive
-// values per thread, and the padding spreads those rows over all banks.
+// the thread's accumulators.  Wb holds sequence qq at Wb[qq * PS + phys(i)]:
+// rows of 16 values whose 16-byte chunks are XOR-swizzled by the row index,
+// so the first pass's 16 consecutive values per thread (vector stores) and
+// the later passes' runs of consecutive values both spread over all banks;
+// FP32 sequences sit 64 bytes apart in bank terms (PS = n + 8) because the
+// first pass interleaves the two sequences of a q block across threads.
 
 template <typename T>
 __device__ __forceinline__ int p2_phys(int i)
 {
-    return i + series_qb<T>() * (i >> 4);
+    if constexpr (sizeof(T) == 4)   // two values per 16-byte chunk
+        return (i & ~15) | ((((i >> 1) & 7) ^ ((i >> 4) & 7)) << 1) | (i & 1);
+    else                            // one value per chunk
+        return (i & ~15) | ((i & 15) ^ ((i >> 4) & 7));
 }
 
-// twiddles w^(r k tstep), r = 1 .. R-1, from the loads of w^(k tstep)
-// x {1, 2, 4, 8} and products of those
+// Twiddles of a pass with Ns > 1: ts[q Ns + k] = w^(2^q k tstep), q < log2 R
+// (built once per block, so a warp's loads hit consecutive k); the other
+// powers are products of those.
 template <typename T, int R>
-__device__ __forceinline__ void p2_twiddle(cplx<T> *v, const cplx<T> *tw, int base)
+__device__ __forceinline__ void p2_twiddle(cplx<T> *v, const cplx<T> *ts, int Ns, int k)
 {
     cplx<T> w[16];
-    w[1] = tw[base];
+    w[1] = ts[k];
     if constexpr (R >= 4) {
-        w[2] = tw[2 * base];
+        w[2] = ts[Ns + k];
         w[3] = cmul(w[1], w[2]);
     }
     if constexpr (R >= 8) {
-        w[4] = tw[4 * base];
+        w[4] = ts[2 * Ns + k];
 #pragma unroll
         for (int r = 5; r < 8; r++) w[r] = cmul(w[r - 4], w[4]);
     }
     if constexpr (R >= 16) {
-        w[8] = tw[8 * base];
+        w[8] = ts[3 * Ns + k];
 #pragma unroll
         for (int r = 9; r < 16; r++) w[r] = cmul(w[r - 8], w[8]);
     }
@@ -191,21 +198,21 @@ __device__ __forceinline__ void p2_load(cplx<T> (&v)[16], const cplx<T> *Wb, int
     }
 }
 
-// twiddles and butterflies of a pass with Ns > 1
+// twiddles and butterflies of a pass with Ns > 1 (ts: the pass's table)
 template <typename T, int R>
-__device__ __forceinline__ void p2_compute(cplx<T> (&v)[16], const cplx<T> *tw, int n, int Ns)
+__device__ __forceinline__ void p2_compute(cplx<T> (&v)[16], const cplx<T> *ts, int n, int Ns)
 {
-    const int m = n / R, tstep = n / (Ns * R);
+    const int m = n / R;
 #pragma unroll
     for (int u = 0; u < 16 / R; u++) {
         const int beta = threadIdx.x + u * blockDim.x;
         const int k = (beta % m) % Ns;
         cplx<T> *x = v + u * R;
-        p2_twiddle<T, R>(x, tw, k * tstep);
+        p2_twiddle<T, R>(x, ts, Ns, k);
         cplx<T> y[R];
 #pragma unroll
         for (int r = 0; r < R; r++) y[r] = x[r];
-        dft_small<T, R>(y, tw, n);
+        dft_small<T, R>(y, ts, n);   // radix 2..16: no table lookups
 #pragma unroll
         for (int r = 0; r < R; r++) x[r] = y[r];
     }
@@ -256,11 +263,21 @@ __device__ __forceinline__ void p2_flush(const T (&a)[16], double *acc, int c, i
 // Last pass (radix R, reads Wb): loads, twiddles, butterflies, accumulate.
 template <typename T, int R>
 __device__ __forceinline__ void p2_last(cplx<T> (&v)[16], T (&a)[16], const cplx<T> *Wb,
-                                        const cplx<T> *tw, int n, int PS, int Ns, T inv_n)
+                                        const cplx<T> *ts, int n, int PS, int Ns, T inv_n)
 {
     p2_load<T, R>(v, Wb, n, PS);
-    p2_compute<T, R>(v, tw, n, Ns);
+    p2_compute<T, R>(v, ts, n, Ns);
     p2_accumulate<T, R>(v, a, inv_n);
+}
+
+// entries of the per-pass twiddle tables for n = 2^log2n
+__host__ __device__ inline int p2_table_size(int log2n)
+{
+    const int n16 = log2n >> 2, lr = log2n & 3;
+    int size = 0, Ns = 16;
+    for (int st = 1; st < n16; st++, Ns *= 16) size += 4 * Ns;
+    if (lr) size += lr * Ns;
+    return size;
 }
 
 // blockIdx.x = c * ntile + tile; a tile is nseq / QB consecutive q blocks
@@ -281,11 +298,12 @@ __global__ void __launch_bounds__(sizeof(T) == 8 ? 256 : 512) time_fft_pow2_kern
     const int c = blockIdx.x / ntile, tile = blockIdx.x % ntile;
     const int qb0 = tile * (nseq / QB);
     const int nblk = min(nseq / QB, nqb - qb0);
-    const int PS = p2_phys<T>(n) + (QB == 2 ? 8 : 0);
+    const int PS = n + (QB == 2 ? 8 : 0);
+    const int n16 = log2n >> 2, rl = 1 << (log2n & 3);
     cplx<T> *S = reinterpret_cast<cplx<T> *>(smem_raw);
     cplx<T> *Wb = S + (size_t)nseq * n;
-    cplx<T> *tw = Wb + (size_t)nseq * PS;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(tw + n);
+    cplx<T> *ts = Wb + (size_t)nseq * PS;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(ts + p2_table_size(log2n));
     __shared__ int abort_flag;
     const uint32_t bar_a = (uint32_t)__cvta_generic_to_shared(bar);
     const uint32_t S_a = (uint32_t)__cvta_generic_to_shared(S);
@@ -316,8 +334,23 @@ __global__ void __launch_bounds__(sizeof(T) == 8 ? 256 : 512) time_fft_pow2_kern
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         issue(0);
     }
-    for (int k = threadIdx.x; k < n; k += blockDim.x) tw[k] = tw_g[k];
-    const int n16 = log2n >> 2, rl = 1 << (log2n & 3);
+    {
+        // per-pass twiddle tables, passes 2 .. nst in order
+        cplx<T> *t = ts;
+        int Ns = 16;
+        for (int st = 1; st <= n16; st++, Ns *= 16) {
+            const int R = st < n16 ? 16 : rl;
+            if (R == 1) break;
+            int nq = 0;
+            while ((1 << nq) < R) nq++;
+            const int tstep = n / (Ns * R);
+            for (int e = threadIdx.x; e < nq * Ns; e += blockDim.x) {
+                const int q = e / Ns, k = e - q * Ns;
+                t[e] = tw_g[(1 << q) * k * tstep];
+            }
+            t += nq * Ns;
+        }
+    }
     const int nst = n16 + (rl > 1 ? 1 : 0);
     const T inv_n = T(1) / T(n);
     T a[16];
@@ -353,7 +386,7 @@ __global__ void __launch_bounds__(sizeof(T) == 8 ? 256 : 512) time_fft_pow2_kern
         }
         __syncthreads();   // S consumed; Wb free (the previous sample's last pass has read it)
         if (threadIdx.x == 0 && s + 1 < W) issue(s + 1);
-        dft_small<T, 16>(v, tw, n);
+        dft_small<T, 16>(v, ts, n);   // no table lookups at radix 16
         if (nst == 1) {
             p2_accumulate<T, 16>(v, a, inv_n);
             continue;
@@ -361,34 +394,37 @@ __global__ void __launch_bounds__(sizeof(T) == 8 ? 256 : 512) time_fft_pow2_kern
         {
             const int m = n / 16;
             const int qi = threadIdx.x % QB, j = (threadIdx.x / QB) % m, blk = threadIdx.x / (QB * m);
-            cplx<T> *dst = Wb + (size_t)(blk * QB + qi) * PS + p2_phys<T>(16 * j);
+            // row j of the swizzled layout: chunk c of the row at c ^ (j & 7)
+            cplx<T> *dst = Wb + (size_t)(blk * QB + qi) * PS + 16 * j;
+            const int sw = j & 7;
             if constexpr (QB == 2) {
 #pragma unroll
                 for (int r = 0; r < 16; r += 2)
-                    *reinterpret_cast<float4 *>(dst + r) = make_float4(
+                    *reinterpret_cast<float4 *>(dst + 2 * ((r >> 1) ^ sw)) = make_float4(
                         (float)v[r].x, (float)v[r].y, (float)v[r + 1].x, (float)v[r + 1].y);
             } else {
 #pragma unroll
                 for (int r = 0; r < 16; r++)
-                    *reinterpret_cast<double2 *>(dst + r) = make_double2((double)v[r].x, (double)v[r].y);
+                    *reinterpret_cast<double2 *>(dst + (r ^ sw)) = make_double2((double)v[r].x, (double)v[r].y);
             }
         }
         __syncthreads();
         int Ns = 16;
-        for (int st = 1; st < n16; st++, Ns *= 16) {
+        const cplx<T> *tp = ts;   // this pass's twiddle table
+        for (int st = 1; st < n16; st++, tp += 4 * Ns, Ns *= 16) {
             if (st == nst - 1) {
-                p2_last<T, 16>(v, a, Wb, tw, n, PS, Ns, inv_n);
+                p2_last<T, 16>(v, a, Wb, tp, n, PS, Ns, inv_n);
             } else {
                 p2_load<T, 16>(v, Wb, n, PS);
                 __syncthreads();
-                p2_compute<T, 16>(v, tw, n, Ns);
+                p2_compute<T, 16>(v, tp, n, Ns);
                 p2_store<T, 16>(v, Wb, n, PS, Ns);
                 __syncthreads();
             }
         }
-        if (rl == 2) p2_last<T, 2>(v, a, Wb, tw, n, PS, Ns, inv_n);
-        else if (rl == 4) p2_last<T, 4>(v, a, Wb, tw, n, PS, Ns, inv_n);
-        else if (rl == 8) p2_last<T, 8>(v, a, Wb, tw, n, PS, Ns, inv_n);
+        if (rl == 2) p2_last<T, 2>(v, a, Wb, tp, n, PS, Ns, inv_n);
+        else if (rl == 4) p2_last<T, 4>(v, a, Wb, tp, n, PS, Ns, inv_n);
+        else if (rl == 8) p2_last<T, 8>(v, a, Wb, tp, n, PS, Ns, inv_n);
     }
     if (abort_flag) {
         // the copy in flight (sample s_abort) lands before the block exits
@@ -502,8 +538,8 @@ static size_t pow2_smem(int n, int nseq, int precision)
 {
     const size_t e = precision == 0 ? sizeof(cplx<double>) : sizeof(cplx<float>);
     const int qb = series_qblock(precision);
-    const size_t ps = (size_t)n + (size_t)qb * (n / 16) + (qb == 2 ? 8 : 0);
-    return ((size_t)nseq * n + (size_t)nseq * ps + n) * e + 16;
+    const size_t ps = (size_t)n + (qb == 2 ? 8 : 0);
+    return ((size_t)nseq * n + (size_t)nseq * ps + p2_table_size(pow2_log2(n))) * e + 16;
 }
 
 // sequences per block of the generic transform: a multiple of the q block,

@@ -134,9 +134,17 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
     constexpr bool NBREG = SPT * (ZT / 2) <= 12;
     uint32_t nbw[NBREG ? SPT : 1][NBREG ? ZT / 2 : 1];
     int pc0[SPT], pc1[SPT];
+    bool own_[SPT], bnd[SPT];
 
     // ---- helpers
     auto cl_sync = [&]() { cl.sync(); };
+    // Split cluster barrier.  A stage ends with arrive (release: this
+    // thread's local stores and halo pushes) and a CTA barrier; the next
+    // stage computes the sites whose neighbours are all own sites first,
+    // then waits (acquire) and computes the sites that read halo copies.
+    // Every thread alternates arrive and wait.
+    auto arrive = [&]() { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); };
+    auto wait = [&]() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); };
 
     // Sum of NV doubles over every thread of every CTA of the cluster; all
     // threads receive the totals, summed in a fixed order.
@@ -354,7 +362,28 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
             for (int j = 0; j < ZT / 2; j++) nbw[k][j] = own ? idx[j * nom + li] : 0u;
         pc0[k] = (own && P.pmax > 0) ? push[li] : -1;
         pc1[k] = (own && P.pmax > 1) ? push[nom + li] : -1;
+        // a site is on the boundary when a neighbour slot is a halo copy
+        bool b = false;
+        if (own)
+            for (int j = 0; j < ZT / 2; j++) {
+                const uint32_t w = idx[j * nom + li];
+                const int s0 = (int)(w & 0xffffu), s1 = (int)(w >> 16);
+                b = b || (s0 >= n_own && s0 < n_own + n_halo) || (s1 >= n_own && s1 < n_own + n_halo);
+            }
+        own_[k] = own;
+        bnd[k] = b;
     }
+    // the sites of the thread whose neighbours are all own sites, the
+    // barrier wait, then the sites that read halo copies
+    auto two_pass = [&](auto &&body) {
+#pragma unroll
+        for (int k = 0; k < SPT; k++)
+            if (own_[k] && !bnd[k]) body(k);
+        wait();
+#pragma unroll
+        for (int k = 0; k < SPT; k++)
+            if (own_[k] && bnd[k]) body(k);
+    };
 
     double E0, drift = 0.0;
     if (J.rec_begin == 0) {
@@ -372,8 +401,8 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
         if (rank == 0 && tid == 0) drift = J.stats[smp * 4 + 0];
     }
     fill(A);
+    arrive();
     __syncthreads();
-    cl_sync();
 
     const T dt = T(J.dt);
     const T f1 = T(1.0 / 6.0), f2 = T(2.0 / 6.0);
@@ -386,88 +415,82 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
             const bool fix = per_step || (n % F == 0);
             double eref = 0.0;
             // ---- stage 1: A -> B
-#pragma unroll
-            for (int k = 0; k < SPT; k++) {
+            two_pass([&](int k) {
                 const int li = tid + k * NT;
-                if (li < n_own) {
-                    T h[3], Sp[3], Pv[3];
-                    field(A, k, li, mk[k], h);
-                    Sp[0] = spin(k, 0);
-                    Sp[1] = spin(k, 1);
-                    Sp[2] = spin(k, 2);
-                    if (sizeof(T) == 8 && per_step)
-                        eref += S[k][0] * h[0] + S[k][1] * h[1] + S[k][2] * h[2] - hz * S[k][2];
-                    Pv[0] = h[1] * Sp[2] - h[2] * Sp[1];
-                    Pv[1] = h[2] * Sp[0] - h[0] * Sp[2];
-                    Pv[2] = h[0] * Sp[1] - h[1] * Sp[0];
+                T h[3], Sp[3], Pv[3];
+                field(A, k, li, mk[k], h);
+                Sp[0] = spin(k, 0);
+                Sp[1] = spin(k, 1);
+                Sp[2] = spin(k, 2);
+                if (sizeof(T) == 8 && per_step)
+                    eref += S[k][0] * h[0] + S[k][1] * h[1] + S[k][2] * h[2] - hz * S[k][2];
+                Pv[0] = h[1] * Sp[2] - h[2] * Sp[1];
+                Pv[1] = h[2] * Sp[0] - h[0] * Sp[2];
+                Pv[2] = h[0] * Sp[1] - h[1] * Sp[0];
 #pragma unroll
-                    for (int c = 0; c < 3; c++) {
-                        const T K = dt * Pv[c];
-                        acc[k][c] = f1 * K;
-                        Pin[k][c] = Sp[c] + T(0.5) * K;
-                    }
-                    const T m = mk[k];
-                    put(B, k, li, {m * Pin[k][0], m * Pin[k][1], m * Pin[k][2], zero});
+                for (int c = 0; c < 3; c++) {
+                    const T K = dt * Pv[c];
+                    acc[k][c] = f1 * K;
+                    Pin[k][c] = Sp[c] + T(0.5) * K;
                 }
-            }
-            cl_sync();
+                const T m = mk[k];
+                put(B, k, li, {m * Pin[k][0], m * Pin[k][1], m * Pin[k][2], zero});
+            });
+            arrive();
+            __syncthreads();
             // ---- stages 2 and 3
 #pragma unroll
             for (int stg = 0; stg < 2; stg++) {
                 const Vec4<T> *src = stg ? A : B;
                 Vec4<T> *dst = stg ? B : A;
                 const T cst = stg ? T(1) : T(0.5);
-#pragma unroll
-                for (int k = 0; k < SPT; k++) {
+                two_pass([&](int k) {
                     const int li = tid + k * NT;
-                    if (li < n_own) {
-                        T h[3], Pv[3];
-                        field(src, k, li, mk[k], h);
-                        const T *Sp = Pin[k];
-                        Pv[0] = h[1] * Sp[2] - h[2] * Sp[1];
-                        Pv[1] = h[2] * Sp[0] - h[0] * Sp[2];
-                        Pv[2] = h[0] * Sp[1] - h[1] * Sp[0];
-                        T nx[3];
-#pragma unroll
-                        for (int c = 0; c < 3; c++) {
-                            const T K = dt * Pv[c];
-                            acc[k][c] += f2 * K;
-                            nx[c] = spin(k, c) + cst * K;
-                        }
-#pragma unroll
-                        for (int c = 0; c < 3; c++) Pin[k][c] = nx[c];
-                        const T m = mk[k];
-                        put(dst, k, li, {m * nx[0], m * nx[1], m * nx[2], zero});
-                    }
-                }
-                cl_sync();
-            }
-            // ---- stage 4 and the FP64 combination
-#pragma unroll
-            for (int k = 0; k < SPT; k++) {
-                const int li = tid + k * NT;
-                if (li < n_own) {
                     T h[3], Pv[3];
-                    field(B, k, li, mk[k], h);
+                    field(src, k, li, mk[k], h);
                     const T *Sp = Pin[k];
                     Pv[0] = h[1] * Sp[2] - h[2] * Sp[1];
                     Pv[1] = h[2] * Sp[0] - h[0] * Sp[2];
                     Pv[2] = h[0] * Sp[1] - h[1] * Sp[0];
-                    double v[3];
+                    T nx[3];
 #pragma unroll
                     for (int c = 0; c < 3; c++) {
-                        acc[k][c] += f1 * (dt * Pv[c]);
-                        v[c] = S[k][c] + (double)acc[k][c];
+                        const T K = dt * Pv[c];
+                        acc[k][c] += f2 * K;
+                        nx[c] = spin(k, c) + cst * K;
                     }
-                    normalise(v);
 #pragma unroll
-                    for (int c = 0; c < 3; c++) S[k][c] = v[c];
-                    sync_spin(k);
-                }
+                    for (int c = 0; c < 3; c++) Pin[k][c] = nx[c];
+                    const T m = mk[k];
+                    put(dst, k, li, {m * nx[0], m * nx[1], m * nx[2], zero});
+                });
+                arrive();
+                __syncthreads();
             }
+            // ---- stage 4 and the FP64 combination (reads B, writes nothing
+            // shared, so no barrier follows)
+            two_pass([&](int k) {
+                T h[3], Pv[3];
+                field(B, k, tid + k * NT, mk[k], h);
+                const T *Sp = Pin[k];
+                Pv[0] = h[1] * Sp[2] - h[2] * Sp[1];
+                Pv[1] = h[2] * Sp[0] - h[0] * Sp[2];
+                Pv[2] = h[0] * Sp[1] - h[1] * Sp[0];
+                double v[3];
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    acc[k][c] += f1 * (dt * Pv[c]);
+                    v[c] = S[k][c] + (double)acc[k][c];
+                }
+                normalise(v);
+#pragma unroll
+                for (int c = 0; c < 3; c++) S[k][c] = v[c];
+                sync_spin(k);
+            });
             if (!fix) {
                 publishA();
-                cl_sync();
+                arrive();
+                __syncthreads();
                 continue;
             }
             // ---- energy correction
@@ -529,10 +552,15 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
                 }
             }
             publishA();   // the reduction's cluster barrier ordered every read of A / D before this
-            cl_sync();
+            arrive();
+            __syncthreads();
         }
+        wait();   // completes the step's barrier before record's own reduction
         record(r);
+        arrive();
+        __syncthreads();
     }
+    wait();
 
     double *stw = J.state + (size_t)smp * 3 * N;
 #pragma unroll

@@ -204,10 +204,9 @@ SMD_API int smd_evolve(smd_ctx *ctx, int lattice_id, int precision, int n_sample
 
 /* ------------------------------------------------------------- serving */
 
-/* Continuous batching: a submitted job is admitted by HBM footprint when
- * memory frees up, its samples are interleaved with other running jobs on
- * the device, and its result is the same as smd_run of the job alone.
- * Inputs are copied at submit; outputs go to the host buffers given at
+/* Job queue: a submitted job is copied, then run by the context's worker
+ * thread in arrival order, each job as smd_run of the job alone (its waves
+ * sized by the HBM budget).  Outputs go to the host buffers given at
  * submit, valid once smd_poll returns SMD_OK. */
 SMD_API int smd_submit(smd_ctx *ctx, const smd_job_desc *job, const double *spins0,
                const double *window, double *spec_out, double *qss_out,
