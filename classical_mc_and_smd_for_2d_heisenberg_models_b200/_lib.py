@@ -69,7 +69,8 @@ class Report(C.Structure):
                 ("site_steps", C.c_double), ("drift_max", C.c_double),
                 ("drift_final", C.c_double), ("waves", C.c_int),
                 ("kernel_launches", C.c_int), ("ms_device", C.c_double), ("ms_rk", C.c_double),
-                ("ms_proj", C.c_double), ("ms_tfft", C.c_double), ("rk_launches", C.c_int)]
+                ("ms_proj", C.c_double), ("ms_tfft", C.c_double), ("rk_launches", C.c_int),
+                ("rk_kind", C.c_int), ("rk_ctas", C.c_int)]
 
 
 _lib = None

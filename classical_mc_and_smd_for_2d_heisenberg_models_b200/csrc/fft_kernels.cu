@@ -469,6 +469,14 @@ __global__ void soa_to_aos_kernel(const double *__restrict__ in, double *__restr
     }
 }
 
+// p[e] *= f
+__global__ void scale_kernel(double *__restrict__ p, size_t n, double f)
+{
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
+         e += (size_t)gridDim.x * blockDim.x)
+        p[e] *= f;
+}
+
 // out[t] += sum_s rows[s][t]
 __global__ void sum_rows_kernel(const double *__restrict__ rows, int W, int n,
                                 double *__restrict__ out)
@@ -622,6 +630,12 @@ cudaError_t launch_aos_to_soa(const double *in, double *out, int W, int N, cudaS
 cudaError_t launch_soa_to_aos(const double *in, double *out, int W, int N, cudaStream_t st)
 {
     soa_to_aos_kernel<<<592, 256, 0, st>>>(in, out, W, N);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scale(double *p, size_t n, double f, cudaStream_t st)
+{
+    scale_kernel<<<1184, 256, 0, st>>>(p, n, f);
     return cudaGetLastError();
 }
 

@@ -19,6 +19,7 @@
 // samples into the job's accumulator.
 #include "../../include/smd_b200.h"
 #include "rk_cluster.cuh"
+#include "rk_rows.cuh"
 #include "smd_launch.h"
 
 #include <cuda_runtime.h>
@@ -80,6 +81,9 @@ struct Lattice {
     std::vector<double> pos;
     std::vector<int> nbr_h[3];      // host copies of the active shells' tables
     std::map<int, std::unique_ptr<ClusterTab>> ctabs;   // keyed by CTAs per sample
+    // row-band kernel: stencil geometry (-2 unchecked, -1 not applicable),
+    // cells per side, active shells
+    int rows_geom = -2, side = 0, rows_shells = 0;
 };
 
 struct QSet {
@@ -520,6 +524,8 @@ struct JobGeom {
     size_t elem, celem;
     ClusterTab *ctab = nullptr;   // cluster kernel partition (null: single-CTA kernel)
     int spt = 0, threads = 0;
+    bool rows = false;            // row-band kernel (takes precedence)
+    RowsParams rp{};
 };
 
 // Partition of lattice L over CS CTAs: contiguous site ranges, halo lists,
@@ -652,15 +658,113 @@ ClusterTab *cluster_tables(Lattice &L, int CS)
 // non-zero couplings) keep the single-CTA kernel.  Otherwise the smallest
 // cluster that puts at least ~85% of the SMs to work is taken, within the
 // shared-memory and register limits; SMD_CLUSTER_CTAS forces a size.
+// Row-band kernel eligibility (rk_rows.cuh): one site per cell
+// (N = side^2, site g = x + side y) and, for every active shell, each
+// site's neighbours at exactly the cell offsets of the square or the
+// triangular stencil.
+void rows_check(Lattice &L)
+{
+    if (L.rows_geom != -2) return;
+    L.rows_geom = -1;
+    const int N = L.N;
+    const int side = (int)std::lround(std::sqrt((double)N));
+    if (side * side != N || side < 6) return;
+    int shells = 0;
+    for (int s = 0; s < 3; s++)
+        if (!L.nbr_h[s].empty() && L.zn[s] > 0) shells |= 1 << s;
+    if (!(shells & 1)) return;
+    for (int geom : {(int)kStencilSquare, (int)kStencilTriang}) {
+        bool ok = true;
+        for (int s = 0; s < 3 && ok; s++) {
+            if (!((shells >> s) & 1)) continue;
+            const int z = L.zn[s];
+            if (z != stencil_z(geom, s)) {
+                ok = false;
+                break;
+            }
+            std::vector<std::pair<int, int>> want(z), got(z);
+            for (int e = 0; e < z; e++) want[e] = {stencil_off(geom, s, e, 0), stencil_off(geom, s, e, 1)};
+            std::sort(want.begin(), want.end());
+            auto wrap = [&](int d) {
+                d = ((d % side) + side) % side;
+                return d >= side / 2 ? d - side : d;
+            };
+            for (int i = 0; i < N && ok; i++) {
+                for (int e = 0; e < z; e++) {
+                    const int j = L.nbr_h[s][(size_t)i * z + e];
+                    if (j < 0 || j >= N) {
+                        ok = false;
+                        break;
+                    }
+                    got[e] = {wrap(j % side - i % side), wrap(j / side - i / side)};
+                }
+                if (!ok) break;
+                std::sort(got.begin(), got.end());
+                ok = got == want;
+            }
+        }
+        if (ok) {
+            L.rows_geom = geom;
+            L.side = side;
+            L.rows_shells = shells;
+            return;
+        }
+    }
+}
+
+// Row bands for the row-band kernel: the smallest band count whose blocks
+// fit the kernel and whose samples x bands fill the SMs (else the largest
+// that fits).  False when the lattice or the form does not fit.
+bool choose_rows(smd_ctx *ctx, JobGeom &g, int n_samples, int sms, int forced)
+{
+    Lattice &L = *g.L;
+    // opt-in (SMD_RK_KERNEL=rows): on the C2 lattice it measured level with
+    // the cluster kernel, which stays the default
+    const char *ke = std::getenv("SMD_RK_KERNEL");
+    if (!(ke && std::strcmp(ke, "rows") == 0)) return false;
+    rows_check(L);
+    if (L.rows_geom < 0 || L.side % rows_spt(g.prec)) return false;
+    bool found = false;
+    for (int CS : {1, 2, 4, 8, 16}) {
+        if (forced && CS != forced) continue;
+        if (L.side / CS < 2) break;
+        RowsParams P{};
+        P.N = L.N;
+        P.L = L.side;
+        P.CS = CS;
+        P.ny_max = 0;
+        for (int r = 0; r <= CS; r++) P.row0[r] = (int)((long long)L.side * r / CS);
+        for (int r = 0; r < CS; r++) P.ny_max = std::max(P.ny_max, P.row0[r + 1] - P.row0[r]);
+        P.geom = L.rows_geom;
+        P.shells = L.rows_shells;
+        P.h = L.dev.h;
+        for (int s = 0; s < 3; s++)
+            for (int c = 0; c < 3; c++) {
+                const bool on = (L.rows_shells >> s) & 1;
+                P.coef64[s][c] = on ? L.dev.coef[s][c] : 0.0;
+                P.coef32[s][c] = (float)P.coef64[s][c];
+            }
+        if (rk_rows_threads(P, g.prec) > rows_max_threads(g.prec)) continue;
+        if (rk_rows_smem(P, g.prec) > 227 * 1024) continue;
+        g.rows = true;
+        g.rp = P;
+        found = true;
+        if (forced || (long long)n_samples * CS >= (long long)(0.85 * sms)) return true;
+    }
+    return found;
+}
+
 void choose_cluster(smd_ctx *ctx, JobGeom &g, int n_samples)
 {
     Lattice &L = *g.L;
     g.ctab = nullptr;
+    g.rows = false;
     if (!L.dev.energy_from_field || L.lieb_delta || !L.vac_only) return;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
     int forced = 0;
     if (const char *e = std::getenv("SMD_CLUSTER_CTAS")) forced = std::atoi(e);
+    if (choose_rows(ctx, g, n_samples, sms, forced)) return;
     const int sizes[] = {1, 2, 4, 8, 16};
     for (int CS : sizes) {
         if (forced && CS != forced) continue;
@@ -707,7 +811,7 @@ int prepare(smd_ctx *ctx, const smd_job_desc *job, JobGeom &g)
     g.prec = job->precision;
     g.nqb = (g.Q + series_qblock(g.prec) - 1) / series_qblock(g.prec);
     choose_cluster(ctx, g, job->n_samples);
-    if (!g.ctab && g.N > rk_max_sites(g.prec))
+    if (!g.rows && !g.ctab && g.N > rk_max_sites(g.prec))
         return fail(ctx, SMD_EINVAL, "job: N exceeds the single-CTA capacity of this form");
     if (g.Qs->use_grid && g.prec == SMD_FP64 && !g.Qs->fp64_ok)
         return fail(ctx, SMD_EINVAL, "job: grid too large for the FP64 shared-memory transform");
@@ -819,7 +923,9 @@ int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const do
             J.stats = ctx->stats.as<double>();
             J.status = ctx->status.as<int>();
             CK(cudaEventRecord(ev(2 + 2 * c), ctx->s_rk), "event");
-            if (g.ctab)
+            if (g.rows)
+                CK(launch_rk_rows(g.rp, J, g.prec, ctx->s_rk), "rk row-band kernel");
+            else if (g.ctab)
                 CK(launch_rk_cluster(g.ctab->P, J, g.prec, g.spt, g.threads, ctx->s_rk), "rk cluster kernel");
             else
                 CK(launch_rk(L.dev, J, g.prec, gen, ctx->s_rk), "rk kernel");
@@ -910,6 +1016,8 @@ int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const do
         rep->ms_proj = ms_proj;
         rep->ms_tfft = ms_tfft;
         rep->rk_launches = rk_launches;
+        rep->rk_kind = g.rows ? 2 : g.ctab ? 1 : 0;
+        rep->rk_ctas = g.rows ? g.rp.CS : g.ctab ? g.ctab->P.CS : 1;
         rep->site_steps = (double)N * (double)(n_rec - 1) * job->stride * job->n_samples;
     }
     if (st & 4) return fail(ctx, SMD_ETIMEOUT, "tensor-core projection: a bounded wait expired");
@@ -972,13 +1080,15 @@ extern "C" int smd_run(smd_ctx *ctx, const smd_job_desc *job, const double *spin
                     rep);
     if (rc) return rc;
     auto w2 = std::chrono::steady_clock::now();
-    CK(cudaMemcpy(spec_out, d_acc, acc_b, cudaMemcpyDeviceToHost), "D2H spec");
-    CK(cudaMemcpy(qss_out, d_q, n * sizeof(double), cudaMemcpyDeviceToHost), "D2H qss");
-    if (out_b) CK(cudaMemcpy(final_out, ctx->out_tmp.p, out_b, cudaMemcpyDeviceToHost), "D2H final");
-    // average over samples, as the reference's fc = 1 / evoCnt (smd_code.cpp:3596-3611)
+    // average over samples on the device, as the reference's fc = 1 / evoCnt
+    // (smd_code.cpp:3596-3611), then one copy of each output
     const double fc = 1.0 / (double)S;
-    for (size_t e = 0; e < 3 * Q * n; e++) spec_out[e] = fc * spec_out[e];
-    for (size_t t = 0; t < n; t++) qss_out[t] = fc * qss_out[t];
+    CK(launch_scale(d_acc, 3 * Q * n + n, fc, ctx->s_rk), "scale");
+    CK(cudaMemcpyAsync(spec_out, d_acc, acc_b, cudaMemcpyDeviceToHost, ctx->s_rk), "D2H spec");
+    CK(cudaMemcpyAsync(qss_out, d_q, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->s_rk), "D2H qss");
+    if (out_b)
+        CK(cudaMemcpyAsync(final_out, ctx->out_tmp.p, out_b, cudaMemcpyDeviceToHost, ctx->s_rk), "D2H final");
+    CK(cudaStreamSynchronize(ctx->s_rk), "sync");
     auto w3 = std::chrono::steady_clock::now();
     if (rep) {
         rep->ms_h2d = std::chrono::duration<double, std::milli>(w1 - w0).count();
@@ -1065,7 +1175,7 @@ extern "C" int smd_evolve(smd_ctx *ctx, int lattice_id, int precision, int n_sam
 }
 
 // ------------------------------------------------------------- serving
-// (filled in by serve.cu)
+// (smd_submit and the rest: serve.cpp)
 
 extern "C" int smd_lattice_sites(smd_ctx *ctx, int lattice_id, int *N)
 {

@@ -136,7 +136,7 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
     for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
-// grid: (row tiles, column tiles).  Rows are snapshot rows of the chunk,
+// grid: (column tiles, row tiles).  Rows are snapshot rows of the chunk,
 // m = (s * R + slot) * 3 + c; rows whose slot >= nrec_chunk are skipped.
 __global__ void __launch_bounds__(128, 1) list_proj_tc_kernel(
     const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
@@ -157,7 +157,9 @@ __global__ void __launch_bounds__(128, 1) list_proj_tc_kernel(
     volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+    // column tiles vary fastest, so the tiles sharing a row tile of A run
+    // together and read it once from HBM
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
     const int total_kb = 3 * nkb;
 
     if (threadIdx.x == 0) {
@@ -346,7 +348,7 @@ cudaError_t launch_list_proj_tc(const CUtensorMap &Ah, const CUtensorMap &Al, co
     auto k = tc::list_proj_tc_kernel;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM);
     if (e != cudaSuccess) return e;
-    dim3 grid((M + tc::BM - 1) / tc::BM, (2 * Lq + tc::BN - 1) / tc::BN);
+    dim3 grid((2 * Lq + tc::BN - 1) / tc::BN, (M + tc::BM - 1) / tc::BM);
     k<<<grid, 128, tc::SMEM, st>>>(Ah, Al, Bh, Bl, M, kp / tc::BK, R, nrec_chunk, rec_begin,
                                    n_rec_total, Lq, win, (cplx<float> *)series, nqb, qoff, status);
     return cudaGetLastError();

@@ -36,6 +36,7 @@ cudaError_t launch_time_fft(const void *series, int precision, int W, int Q, int
 cudaError_t launch_aos_to_soa(const double *in, double *out, int W, int N, cudaStream_t st);
 cudaError_t launch_soa_to_aos(const double *in, double *out, int W, int N, cudaStream_t st);
 cudaError_t launch_sum_rows(const double *rows, int W, int n, double *out, cudaStream_t st);
+cudaError_t launch_scale(double *p, size_t n, double f, cudaStream_t st);
 
 // tensor-core list projection (proj_tc.cu)
 bool make_bf16_map(CUtensorMap *map, const void *base, int rows, int kp, int box_rows);

@@ -165,6 +165,8 @@ typedef struct {
     double ms_proj;        /* summed duration of the projection launches */
     double ms_tfft;        /* summed duration of the time-transform launches */
     int rk_launches;       /* RK kernel launches */
+    int rk_kind;           /* RK kernel used: 0 single-CTA, 1 cluster, 2 row-band */
+    int rk_ctas;           /* CTAs per sample (cluster size) */
 } smd_report;
 
 /* Run a job end to end from host buffers.

@@ -190,10 +190,80 @@ def test_tensor_core_projection_matches_grid_fft(ctx, N_L):
 
 @pytest.fixture
 def cluster_size(monkeypatch):
-    """Force the number of CTAs a sample is spread over (SMD_CLUSTER_CTAS)."""
+    """Force the cluster kernel (SMD_RK_KERNEL) and the number of CTAs a
+    sample is spread over (SMD_CLUSTER_CTAS)."""
     def set_(cs):
+        monkeypatch.setenv("SMD_RK_KERNEL", "cluster")
         monkeypatch.setenv("SMD_CLUSTER_CTAS", str(cs))
     return set_
+
+
+@pytest.fixture
+def row_bands(monkeypatch):
+    """Force the row-band kernel (it is the FP32 form's default; the FP64
+    form takes it on request) and its number of row bands (CTAs per sample)."""
+    def set_(cs):
+        monkeypatch.setenv("SMD_RK_KERNEL", "rows")
+        monkeypatch.setenv("SMD_CLUSTER_CTAS", str(cs))
+    return set_
+
+
+@pytest.mark.parametrize("cs", [1, 2, 4])
+@pytest.mark.parametrize("name", ["traj_square_j1j2", "traj_square_xxz_h_vac", "traj_triang_j1j2"])
+def test_row_band_kernel_200_steps_per_spin(ctx, row_bands, cs, name):
+    """The row-band kernel (square / triangular lattices as padded 2D grids,
+    ghost rows exchanged through distributed shared memory) keeps the
+    reference's per-spin parity."""
+    s, d = load_golden(name)
+    if s.L // cs < 2:
+        pytest.skip("fewer than two rows per band")
+    row_bands(cs)
+    lat, lid = _upload(ctx, s)
+    n = int(d["n"])
+    imp = None if "imp" not in d else np.tile(d["imp"], (n, 1))
+    sp = np.array(d["spins0"][:n], np.float64)
+    qid = ctx.qset(lid)
+    r = ctx.run(lid, qid, sp, s.dtm, 2, stride=s.ntm - 1, imp=imp)
+    assert r.report["rk_kind"] == 2 and r.report["rk_ctas"] == cs, r.report
+    assert np.max(np.abs(r.final - d["final"])) <= SPIN_TOL
+
+
+@pytest.mark.parametrize("cs", [1, 2, 4])
+def test_row_band_fp32_form_tracks_fp64(ctx, row_bands, cs):
+    """FP32 precision form on the row-band kernel (XXZ, field, three shells,
+    vacancies): spectrum within 1e-3 (rel-L2) of the FP64 form, energy drift
+    within 1e-8 per site."""
+    row_bands(cs)
+    s = SMDSettings(geom="square", L=24, J2=0.55, JX=0.1, zlamb1=0.9, zlamb2=0.9, h=0.3,
+                    imp_ratio=0.05, dtm=0.01, ntm=128, NMeas=4000)
+    lat, lid = _upload(ctx, s)
+    qid = ctx.qset(lid)
+    spins, imp = smp.make_samples(s, 4, "stripe", 0.1, 5)
+    impr = np.tile(imp[0], (4, 1))
+    win = smd.window("hann1", 128)
+    r64 = ctx.run(lid, qid, spins, s.dtm, 128, stride=4, win=win, imp=impr)
+    r32 = ctx.run(lid, qid, spins, s.dtm, 128, stride=4, win=win, imp=impr,
+                  precision=_lib.SMD_FP32, fix_every=16)
+    assert r32.report["rk_kind"] == 2 and r64.report["rk_kind"] == 2
+    rel = np.linalg.norm(r32.spec - r64.spec) / np.linalg.norm(r64.spec)
+    assert rel <= 1e-3, rel
+    assert r32.report["drift_max"] <= 1e-8 and r32.report["drift_final"] <= 1e-8
+
+
+def test_row_band_and_cluster_kernels_agree(ctx, monkeypatch):
+    """Triangular L = 48 (the C2 lattice), FP64: both kernels integrate the
+    same trajectory to rounding."""
+    s = SMDSettings(geom="triang", L=48, J2=0.12, dtm=0.02, ntm=64)
+    lat, lid = _upload(ctx, s)
+    qid = ctx.qset(lid)
+    spins, _ = smp.make_samples(s, 3, "q120", 0.15, 7)
+    monkeypatch.setenv("SMD_RK_KERNEL", "cluster")
+    a = ctx.run(lid, qid, spins, s.dtm, 64, stride=4)
+    monkeypatch.setenv("SMD_RK_KERNEL", "rows")
+    b = ctx.run(lid, qid, spins, s.dtm, 64, stride=4)
+    assert a.report["rk_kind"] == 1 and b.report["rk_kind"] == 2
+    assert np.max(np.abs(a.final - b.final)) <= 1e-11
+    assert np.max(np.abs(a.spec - b.spec)) <= 1e-10 * np.max(np.abs(a.spec))
 
 
 @pytest.mark.parametrize("cs", [1, 2, 4, 8])
