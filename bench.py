@@ -35,6 +35,19 @@ METRIC = "SMD site-steps/s"
 UNIT = "site-steps/s"
 
 
+def profile_traffic(name: str):
+    """DRAM bytes (read + write) per launch of a kernel from its committed
+    ncu summary in profiles/ (the `dram_bytes_per_launch:` line), or None."""
+    path = os.path.join(ROOT, "profiles", name)
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_launch:"):
+                return int(line.split(":")[1]), f"profiles/{name}"
+    except OSError:
+        pass
+    return None, None
+
+
 def flops_per_site_step(z: int) -> int:
     """Algorithmic flops of one site-step of RK4 + energy correction: 6 field
     sweeps x 6z, 4 stages x 18, combine and normalise 24, correction 53,
@@ -214,6 +227,8 @@ def run_ours(args, w, rank, world):
     ms_dev = sum(r.ms_device for r in reps)
     ms_rk = sum(r.ms_rk for r in reps)
     rk_launches = sum(r.rk_launches for r in reps)
+    rk_kind = {0: "rk_fp32_kernel" if w.precision == _lib.SMD_FP32 else "rk_fp64_kernel",
+               1: "rk_cluster_kernel", 2: "rk_rows_kernel"}[reps[-1].rk_kind]
     launches = sum(r.kernel_launches for r in reps)
     drift_max = max(r.drift_max for r in reps)
     drift_final = max(r.drift_final for r in reps)
@@ -278,7 +293,8 @@ def run_ours(args, w, rank, world):
     prec_peak = lib.smd_measure_fma_peak(local, w.precision, C.byref(peak))
     rk_flops = fpss * site_steps_rank * args.steps
     achieved = rk_flops / (ms_rk / 1e3) / 1e12
-    roof = {"kernel": "rk_fp32_kernel" if w.precision == _lib.SMD_FP32 else "rk_fp64_kernel",
+    traffic, traffic_src = profile_traffic(f"{rk_kind}_{w.name}.md")
+    roof = {"kernel": rk_kind,
             "bound": "fp32" if w.precision == _lib.SMD_FP32 else "fp64",
             "achieved": achieved, "peak": peak.value if prec_peak == 0 else None,
             "unit": "TFLOP/s",
@@ -286,7 +302,8 @@ def run_ours(args, w, rank, world):
             "peak_source": "smd_measure_fma_peak (FMA chains on every SM)",
             "algorithmic_flops_per_site_step": fpss,
             "avg_launch_ms": ms_rk / max(1, rk_launches),
-            "traffic": None}
+            "traffic": traffic, "traffic_unit": "bytes per launch (DRAM read + write)",
+            "traffic_source": traffic_src}
 
     if dist is not None:
         dist.destroy_process_group()
