@@ -114,6 +114,58 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+# ------------------------------------------------------------- serving
+
+def serving_leg(ctx, n_jobs: int, seed: int):
+    """A bounded stream of serving-workload jobs (workloads.c5_stream) through
+    the job queue (smd_submit / smd_wait): one burst to measure the queue's
+    service capacity, then Poisson arrivals at 70 % of it; latency = submit
+    to completion as the library measures it."""
+    from classical_mc_and_smd_for_2d_heisenberg_models_b200 import smd, workloads
+    jobs = workloads.c5_stream(n_jobs, seed)
+    prepared = []
+    for w in jobs:
+        s = w.settings
+        lat = smd.build_lattice(s.geom, s.L)
+        lid = ctx.lattice(s, lat)
+        qid = ctx.qset(lid)
+        spins, imp = workloads.make_inputs(w)
+        imp_arr = None if imp is None else np.ascontiguousarray(imp, np.int32)
+        win = smd.window(w.window, w.n_rec)
+        prepared.append((w, lid, qid, spins, imp_arr, win))
+    site_steps = sum(w.settings.N * w.n_samples * w.steps for w, *_ in prepared)
+
+    def submit(p):
+        w, lid, qid, spins, imp_arr, win = p
+        return ctx.submit(lid, qid, spins, w.settings.dtm, w.n_rec, stride=w.stride,
+                          precision=w.precision, fix_every=w.fix_every, win=win, imp=imp_arr)
+
+    # burst: every job queued at once; the largest latency is the makespan
+    ids = [submit(p) for p in prepared]
+    lat = [ctx.wait(j)[2] for j in ids]
+    makespan_ms = max(lat)
+    rate = 0.7 * len(prepared) / (makespan_ms / 1e3)
+    rng = np.random.default_rng(seed + 1)
+    gaps = rng.exponential(1.0 / rate, size=len(prepared))
+    t0 = time.perf_counter()
+    ids, t_next = [], 0.0
+    for p, g in zip(prepared, gaps):
+        t_next += g
+        dt = t0 + t_next - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        ids.append(submit(p))
+    lat = np.array([ctx.wait(j)[2] for j in ids])
+    wall = time.perf_counter() - t0
+    return {"jobs": len(prepared), "arrivals": "Poisson", "rate_jobs_per_s": rate,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "max_ms": float(lat.max()), "burst_site_steps_per_s": site_steps / (makespan_ms / 1e3),
+            "sample": f"{len(prepared)} jobs of the serving mix (5 geometries, N log-uniform in "
+                      f"[256, 4096], 16-48 samples, 4092 RK steps at stride 4, 0-10 % vacancies, "
+                      f"grid q, FP32 form), Poisson at 70 % of the burst service rate; "
+                      f"stream wall time {wall:.1f} s"}
+
+
 # --------------------------------------------------------- CPU reference
 
 def reference_runner_step(w, procs: int, ntm: int, workdir: str):
@@ -266,6 +318,11 @@ def run_ours(args, w, rank, world):
     if dist is not None:
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
     e2e_value = site_steps_rank * world / float(tt.item())
+
+    # ---- serving: bounded job stream with p50 / p99 latency (rank 0's queue)
+    serving = None
+    if rank == 0 and not args.no_serving:
+        serving = serving_leg(ctx, args.serving_jobs, 0x5eed05)
     h2d = spins.nbytes + win.nbytes
     d2h = 3 * Q * n * 8 + n * 8
 
@@ -329,6 +386,7 @@ def run_ours(args, w, rank, world):
             "energy_drift_per_site": {"max": drift_max, "final": drift_final},
             "fp64_plain": fp64,
             "speedup_vs_fp64_plain": (value / fp64["value"]) if fp64 else None,
+            "serving": serving,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": float(tt.item()) * 1e3},
             "roofline": roof,
@@ -390,6 +448,8 @@ def main():
     ap.add_argument("--ref-ntm", type=int, default=1025)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serving-jobs", type=int, default=24)
     ap.add_argument("--records", type=int, default=0,
                     help="override the record count (small profiling cases only)")
     ap.add_argument("--samples", type=int, default=0,

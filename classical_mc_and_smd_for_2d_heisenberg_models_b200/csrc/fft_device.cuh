@@ -167,39 +167,41 @@ __device__ __forceinline__ void stockham_stage(cplx<T> *buf, int n, int nseq, in
 
 // Any other radix: one butterfly at a time, streaming from a copy of the
 // sequences.  Kept out of line so that its register needs stay apart from
-// the radix-4 / radix-2 path; thread mapping as in stockham_stage.
+// the inline stages.  The copy holds up to scr_seqs sequences ([seq][x],
+// compact), so the sequences go through it in batches; thread mapping as in
+// stockham_stage.
 template <typename T>
 __device__ __noinline__ void stockham_stage_generic(cplx<T> *buf, int n, int nseq, int ss, int es,
                                                     int Ns, int R, const cplx<T> *tw,
-                                                    cplx<T> *scratch)
+                                                    cplx<T> *scratch, int scr_seqs)
 {
-    // scratch: a copy of the sequences (same layout), so loads and stores
-    // touch different arrays
     const bool qfast = es != 1 || (ss & 1);
-    const int total = nseq * n;
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
-        const int q = qfast ? e % nseq : e / n;
-        const int x = qfast ? e / nseq : e - q * n;
-        scratch[q * ss + x * es] = buf[q * ss + x * es];
-    }
-    __syncthreads();
-    const int m = n / R, nb = nseq * m, tstep = n / (Ns * R);
-    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-        const int q = qfast ? b % nseq : b / m;
-        const int j = qfast ? b / nseq : b - q * m;
-        const int k = j % Ns;
-        const int idx = (j / Ns) * Ns * R + k;
-        for (int p = 0; p < R; p++) {
-            cplx<T> s = {T(0), T(0)};
-            for (int r = 0; r < R; r++) {
-                cplx<T> x = scratch[q * ss + (j + r * m) * es];
-                if (r) x = cmul(x, tw[(r * k) * tstep]);   // index < n
-                s = cadd(s, cmul(x, tw[((r * p) % R) * (n / R)]));
-            }
-            buf[q * ss + (idx + p * Ns) * es] = s;
+    const int m = n / R, tstep = n / (Ns * R);
+    for (int q0 = 0; q0 < nseq; q0 += scr_seqs) {
+        const int nq = min(scr_seqs, nseq - q0);
+        for (int e = threadIdx.x; e < nq * n; e += blockDim.x) {
+            const int qq = qfast ? e % nq : e / n;
+            const int x = qfast ? e / nq : e - qq * n;
+            scratch[qq * n + x] = buf[(q0 + qq) * ss + x * es];
         }
+        __syncthreads();
+        for (int b = threadIdx.x; b < nq * m; b += blockDim.x) {
+            const int qq = qfast ? b % nq : b / m;
+            const int j = qfast ? b / nq : b - qq * m;
+            const int k = j % Ns;
+            const int idx = (j / Ns) * Ns * R + k;
+            for (int p = 0; p < R; p++) {
+                cplx<T> s = {T(0), T(0)};
+                for (int r = 0; r < R; r++) {
+                    cplx<T> x = scratch[qq * n + j + r * m];
+                    if (r) x = cmul(x, tw[(r * k) * tstep]);   // index < n
+                    s = cadd(s, cmul(x, tw[((r * p) % R) * (n / R)]));
+                }
+                buf[(q0 + qq) * ss + (idx + p * Ns) * es] = s;
+            }
+        }
+        __syncthreads();
     }
-    __syncthreads();
 }
 
 // Stage sets a transform kernel is built with (FL flags), so that each plan
@@ -214,7 +216,7 @@ enum { FK_R3 = 1, FK_GEN = 2, FK_R16 = 4 };
 // nseq * n <= C * blockDim.x.
 template <typename T, int C, int FL>
 __device__ void smem_fft(cplx<T> *buf, int n, int nseq, int ss, int es, const int *radix,
-                         int nst, const cplx<T> *tw, cplx<T> *scratch)
+                         int nst, const cplx<T> *tw, cplx<T> *scratch, int scr_seqs)
 {
     int Ns = 1;
     for (int s = 0; s < nst; s++) {
@@ -235,7 +237,8 @@ __device__ void smem_fft(cplx<T> *buf, int n, int nseq, int ss, int es, const in
                     break;
                 }
             }
-            if constexpr ((FL & FK_GEN) != 0) stockham_stage_generic<T>(buf, n, nseq, ss, es, Ns, R, tw, scratch);
+            if constexpr ((FL & FK_GEN) != 0)
+                stockham_stage_generic<T>(buf, n, nseq, ss, es, Ns, R, tw, scratch, scr_seqs);
             break;
         }
         Ns *= R;

@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(1024) time_fft_kernel(
             buf[(b * QB + qi) * n + t] = src[e];
         }
         __syncthreads();
-        smem_fft<T, MAXA, FL>(buf, n, QT, n, 1, plan.radix, plan.nst, tw_g, scratch);
+        smem_fft<T, MAXA, FL>(buf, n, QT, n, 1, plan.radix, plan.nst, tw_g, scratch, QT);
 #pragma unroll
         for (int u = 0; u < MAXA; u++) {
             const int e = threadIdx.x + u * blockDim.x;

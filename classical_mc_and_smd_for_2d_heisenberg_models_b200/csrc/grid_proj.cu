@@ -20,6 +20,8 @@
 // ...), the others the runtime plan.
 #include "fft_device.cuh"
 
+#include <algorithm>
+
 namespace smd {
 
 // two-stage transform with compile-time radices P1 then P2 (P2 = 1: none)
@@ -38,7 +40,8 @@ template <typename TS, typename T, int FL, int P1, int P2, int MAXT, int MINB>
 __global__ void __launch_bounds__(MAXT, MINB) grid_proj_kernel(
     const TS *__restrict__ snap, int N, int R, int nrec_chunk, int rec_begin, int n_rec_total,
     const int *__restrict__ grid_map, FFTPlan plan, const cplx<T> *__restrict__ tw_g,
-    double scale, const double *__restrict__ win, cplx<T> *__restrict__ series, int nqb, int NG)
+    double scale, const double *__restrict__ win, cplx<T> *__restrict__ series, int nqb, int NG,
+    int scr_seqs)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int QB = series_qb<T>();
@@ -70,8 +73,8 @@ __global__ void __launch_bounds__(MAXT, MINB) grid_proj_kernel(
         smem_fft_fixed<T, 16, P1, P2>(buf, G, NG * G, P, 1, tw);        // rows
         smem_fft_fixed<T, 16, P1, P2>(buf, G, NG * P - 1, 1, NG * P, tw);   // columns
     } else {
-        smem_fft<T, 16, FL>(buf, G, NG * G, P, 1, plan.radix, plan.nst, tw, scratch);
-        smem_fft<T, 16, FL>(buf, G, NG * P - 1, 1, NG * P, plan.radix, plan.nst, tw, scratch);
+        smem_fft<T, 16, FL>(buf, G, NG * G, P, 1, plan.radix, plan.nst, tw, scratch, scr_seqs);
+        smem_fft<T, 16, FL>(buf, G, NG * P - 1, 1, NG * P, plan.radix, plan.nst, tw, scratch, scr_seqs);
     }
     const int t0 = rec_begin + slot0;
     const T sc0 = T(scale * win[t0]), sc1 = has1 ? T(scale * win[t0 + 1]) : T(0);
@@ -110,14 +113,126 @@ __global__ void __launch_bounds__(MAXT, MINB) grid_proj_kernel(
     }
 }
 
+// ---------------------------------------------------------- large grids
+//
+// Grids too large for one block (G up to 512) take two passes through a
+// global scratch Zg [W][pairs][3][G][G] of the packed complex grids:
+// rows first (RT rows per block), then columns.  A column block transforms
+// CT columns kc and their mirrors (G - kc) % G, which the Hermitian
+// separation of the two records needs, and writes the series as the
+// one-block kernel does.
+
+// blockIdx.x = (pair * 3 + c) * row_tiles + tile, blockIdx.y = sample
+template <typename TS, typename T, int FL>
+__global__ void __launch_bounds__(512) grid_rows_kernel(
+    const TS *__restrict__ snap, int N, int R, int nrec_chunk, const int *__restrict__ grid_map,
+    FFTPlan plan, const cplx<T> *__restrict__ tw_g, cplx<T> *__restrict__ Zg, int RT,
+    int scr_seqs)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int G = plan.n, P = G + 1;
+    const int tiles = (G + RT - 1) / RT;
+    const int tile = blockIdx.x % tiles, pc = blockIdx.x / tiles;
+    const int c = pc % 3, pair = pc / 3, s = blockIdx.y;
+    const int r0 = tile * RT, nr = min(RT, G - r0);
+    cplx<T> *buf = reinterpret_cast<cplx<T> *>(smem_raw);
+    cplx<T> *tw = buf + (size_t)RT * P;
+    cplx<T> *scratch = (FL & FK_GEN) ? tw + G : nullptr;
+    const int slot0 = 2 * pair;
+    const bool has1 = slot0 + 1 < nrec_chunk;
+    const TS *x0 = snap + ((size_t)(s * R + slot0) * 3 + c) * N;
+    const TS *x1 = x0 + 3 * (size_t)N;
+    for (int k = threadIdx.x; k < G; k += blockDim.x) tw[k] = tw_g[k];
+    for (int e = threadIdx.x; e < RT * G; e += blockDim.x) {
+        const int rr = e / G, col = e - rr * G;
+        T a = T(0), b = T(0);
+        if (rr < nr) {
+            const int idx = grid_map[(r0 + rr) * G + col];
+            if (idx >= 0) {
+                a = T(x0[idx]);
+                if (has1) b = T(x1[idx]);
+            }
+        }
+        buf[rr * P + col] = {a, b};
+    }
+    __syncthreads();
+    smem_fft<T, 8, FL>(buf, G, RT, P, 1, plan.radix, plan.nst, tw, scratch, scr_seqs);
+    cplx<T> *z = Zg + (((size_t)s * ((R + 1) / 2) + pair) * 3 + c) * G * G;
+    for (int e = threadIdx.x; e < nr * G; e += blockDim.x) {
+        const int rr = e / G, col = e - rr * G;
+        z[(size_t)(r0 + rr) * G + col] = buf[rr * P + col];
+    }
+}
+
+// blockIdx.x = (pair * 3 + c) * col_tiles + tile, blockIdx.y = sample
+template <typename T, int FL>
+__global__ void __launch_bounds__(512) grid_cols_kernel(
+    int R, int nrec_chunk, int rec_begin, int n_rec_total, FFTPlan plan,
+    const cplx<T> *__restrict__ tw_g, const cplx<T> *__restrict__ Zg, double scale,
+    const double *__restrict__ win, cplx<T> *__restrict__ series, int nqb, int CT, int scr_seqs)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int QB = series_qb<T>();
+    const int G = plan.n, W2 = 2 * CT, Pw = W2 + 1;   // element pitch (odd)
+    const int tiles = (G + CT - 1) / CT;
+    const int tile = blockIdx.x % tiles, pc = blockIdx.x / tiles;
+    const int c = pc % 3, pair = pc / 3, s = blockIdx.y;
+    const int c0 = tile * CT;
+    cplx<T> *buf = reinterpret_cast<cplx<T> *>(smem_raw);    // [G][Pw]
+    cplx<T> *tw = buf + (size_t)G * Pw;
+    cplx<T> *scratch = (FL & FK_GEN) ? tw + G : nullptr;
+    const int slot0 = 2 * pair;
+    const bool has1 = slot0 + 1 < nrec_chunk;
+    const cplx<T> *z = Zg + (((size_t)s * ((R + 1) / 2) + pair) * 3 + c) * G * G;
+    for (int k = threadIdx.x; k < G; k += blockDim.x) tw[k] = tw_g[k];
+    // columns j < CT: kc = c0 + j; columns CT + j: their mirrors
+    for (int e = threadIdx.x; e < G * W2; e += blockDim.x) {
+        const int x = e / W2, j = e - x * W2;
+        const int jj = j < CT ? j : j - CT;
+        int kc = min(c0 + jj, G - 1);
+        if (j >= CT) kc = kc ? G - kc : 0;
+        buf[x * Pw + j] = z[(size_t)x * G + kc];
+    }
+    __syncthreads();
+    smem_fft<T, 8, FL>(buf, G, W2, 1, Pw, plan.radix, plan.nst, tw, scratch, scr_seqs);
+    const int t0 = rec_begin + slot0;
+    const T sc0 = T(scale * win[t0]), sc1 = has1 ? T(scale * win[t0 + 1]) : T(0);
+    const int nb = (CT + QB - 1) / QB;   // q blocks of a row in this tile
+    for (int e = threadIdx.x; e < G * nb; e += blockDim.x) {
+        const int kr = e / nb, jb = e - kr * nb;
+        const int nr = kr ? G - kr : 0;
+        cplx<T> o0[QB], o1[QB];
+        bool ok = true;
+#pragma unroll
+        for (int i = 0; i < QB; i++) {
+            const int j = jb * QB + i;
+            ok = ok && (j < CT) && (c0 + j < G);
+            const int jc = min(j, CT - 1);
+            const cplx<T> zz = buf[kr * Pw + jc], zm = buf[nr * Pw + CT + jc];
+            o0[i] = {sc0 * T(0.5) * (zz.x + zm.x), sc0 * T(0.5) * (zz.y - zm.y)};
+            o1[i] = {sc1 * T(0.5) * (zz.y + zm.y), sc1 * T(-0.5) * (zz.x - zm.x)};
+        }
+        if (!ok) continue;
+        const int q = kr * G + c0 + jb * QB;   // q and q + 1 share a block (G, c0, CT even)
+        cplx<T> *out = series + ((((size_t)s * 3 + c) * nqb + q / QB) * n_rec_total + t0) * QB;
+#pragma unroll
+        for (int i = 0; i < QB; i++) {
+            out[i] = o0[i];
+            if (has1) out[QB + i] = o1[i];
+        }
+    }
+}
+
 // ---------------------------------------------------------- launchers
 
 namespace {
 
 using GridKernelF = void (*)(const float *, int, int, int, int, int, const int *, FFTPlan,
-                             const cplx<float> *, double, const double *, cplx<float> *, int, int);
+                             const cplx<float> *, double, const double *, cplx<float> *, int, int,
+                             int);
 using GridKernelD = void (*)(const double *, int, int, int, int, int, const int *, FFTPlan,
-                             const cplx<double> *, double, const double *, cplx<double> *, int, int);
+                             const cplx<double> *, double, const double *, cplx<double> *, int, int,
+                             int);
 
 // compile-time plans: (P1, P2) for G = P1 * P2
 template <typename T, int P1, int P2>
@@ -162,26 +277,106 @@ auto pick_kernel(const FFTPlan &p)
 // values a column pass of NG components transforms
 static size_t grid_work(int G, int ng) { return (size_t)G * ((size_t)ng * (G + 1) - 1); }
 
+// sequences of length G the out-of-line stage's copy holds (at most 4096
+// values, at least one sequence); 0 for plans without such a stage
+static int grid_scratch_seqs(int G, int ng, const FFTPlan &p)
+{
+    if (!plan_generic(p)) return 0;
+    const size_t all = (size_t)ng * (G + 1);
+    const size_t cap = std::max<size_t>(1, 4096 / (size_t)G);
+    return (int)std::min(all, cap);
+}
+
 // Components per block: all three while their values fit 512 threads of
 // 16 values and the shared memory of two blocks per SM (FP32) or one (FP64),
 // else one.  0: the grid does not fit one block.
-int grid_proj_ng(int G, int precision, const FFTPlan &p)
+static size_t grid_smem_ng(int G, int ng, int precision, const FFTPlan &p)
 {
     const size_t e = precision == 0 ? sizeof(cplx<double>) : sizeof(cplx<float>);
-    const size_t mult = plan_generic(p) ? 2 : 1;
-    const size_t GP = (size_t)G * (G + 1);
+    return ((size_t)ng * G * (G + 1) + G + (size_t)grid_scratch_seqs(G, ng, p) * G) * e;
+}
+
+int grid_proj_ng(int G, int precision, const FFTPlan &p)
+{
     const size_t cap3 = (precision == 0 ? 200 : 110) * 1024;
-    if (grid_work(G, 3) <= 16 * 512 && 3 * GP * e * mult + G * e <= cap3) return 3;
-    if (grid_work(G, 1) <= 16 * 1024 && GP * e * mult + G * e <= 200 * 1024) return 1;
+    if (grid_work(G, 3) <= 16 * 512 && grid_smem_ng(G, 3, precision, p) <= cap3) return 3;
+    if (grid_work(G, 1) <= 16 * 1024 && grid_smem_ng(G, 1, precision, p) <= 200 * 1024) return 1;
     return 0;
 }
 
 size_t grid_proj_smem(int G, int precision, const FFTPlan &p)
 {
-    const size_t e = precision == 0 ? sizeof(cplx<double>) : sizeof(cplx<float>);
     const int ng = grid_proj_ng(G, precision, p);
-    const size_t GP = (size_t)G * (G + 1) * (ng ? ng : 1);
-    return (GP + G + (plan_generic(p) ? GP : 0)) * e;
+    return grid_smem_ng(G, ng ? ng : 1, precision, p);
+}
+
+// tile sizes of the two-pass path: rows per row block, columns per column
+// block (even, with their mirrors 2 CT columns), about 2048 values each,
+// transformed with 8 values per thread by at most 512 threads
+static int large_rt(int G) { return std::max(1, std::min(G, 2048 / G)); }
+static int large_ct(int G) { return std::max(2, std::min(G, 1024 / G) & ~1); }
+
+static size_t large_smem(int G, int n_values, int precision, const FFTPlan &p, int *scr)
+{
+    const size_t e = precision == 0 ? sizeof(cplx<double>) : sizeof(cplx<float>);
+    *scr = plan_generic(p) ? std::max(1, 4096 / G) : 0;
+    return ((size_t)n_values + G + (size_t)*scr * G) * e;
+}
+
+bool grid_large_ok(int G, int precision, const FFTPlan &p)
+{
+    if (G > 512 || (G & 1)) return false;
+    int scr;
+    const size_t a = large_smem(G, large_rt(G) * (G + 1), precision, p, &scr);
+    const size_t b = large_smem(G, G * (2 * large_ct(G) + 1), precision, p, &scr);
+    return std::max(a, b) <= 200 * 1024 && (size_t)G * (2 * large_ct(G) + 1) <= 8 * 512 &&
+           (size_t)large_rt(G) * (G + 1) <= 8 * 512;
+}
+
+size_t grid_large_scratch(int G, int R, int precision)
+{
+    const size_t e = precision == 0 ? sizeof(cplx<double>) : sizeof(cplx<float>);
+    return (size_t)((R + 1) / 2) * 3 * G * G * e;   // per sample
+}
+
+cudaError_t launch_grid_proj_large(const void *snap, int precision, int N, int W, int R,
+                                   int nrec_chunk, int rec_begin, int n_rec_total,
+                                   const int *grid_map, const FFTPlan &plan, const void *tw,
+                                   double scale, const double *win, void *series, int nqb,
+                                   void *Zg, cudaStream_t st)
+{
+    const int G = plan.n, RT = large_rt(G), CT = large_ct(G);
+    const int pairs = (nrec_chunk + 1) / 2;
+    int scr_r, scr_c;
+    const size_t sm_r = large_smem(G, RT * (G + 1), precision, plan, &scr_r);
+    const size_t sm_c = large_smem(G, G * (2 * CT + 1), precision, plan, &scr_c);
+    const int thr_r = fft_threads(RT * (G + 1), 8), thr_c = fft_threads(G * (2 * CT + 1), 8);
+    const dim3 gr(pairs * 3 * ((G + RT - 1) / RT), W), gc(pairs * 3 * ((G + CT - 1) / CT), W);
+    const bool gen = plan_generic(plan);
+    if (precision == 0) {
+        auto kr = gen ? grid_rows_kernel<double, double, FK_R16 | FK_R3 | FK_GEN>
+                      : grid_rows_kernel<double, double, FK_R16 | FK_R3>;
+        auto kc = gen ? grid_cols_kernel<double, FK_R16 | FK_R3 | FK_GEN> : grid_cols_kernel<double, FK_R16 | FK_R3>;
+        cudaFuncSetAttribute(kr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_r);
+        cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_c);
+        kr<<<gr, thr_r, sm_r, st>>>((const double *)snap, N, R, nrec_chunk, grid_map, plan,
+                                    (const cplx<double> *)tw, (cplx<double> *)Zg, RT, scr_r);
+        kc<<<gc, thr_c, sm_c, st>>>(R, nrec_chunk, rec_begin, n_rec_total, plan, (const cplx<double> *)tw,
+                                    (const cplx<double> *)Zg, scale, win, (cplx<double> *)series, nqb, CT,
+                                    scr_c);
+    } else {
+        auto kr = gen ? grid_rows_kernel<float, float, FK_R16 | FK_R3 | FK_GEN>
+                      : grid_rows_kernel<float, float, FK_R16 | FK_R3>;
+        auto kc = gen ? grid_cols_kernel<float, FK_R16 | FK_R3 | FK_GEN> : grid_cols_kernel<float, FK_R16 | FK_R3>;
+        cudaFuncSetAttribute(kr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_r);
+        cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_c);
+        kr<<<gr, thr_r, sm_r, st>>>((const float *)snap, N, R, nrec_chunk, grid_map, plan,
+                                    (const cplx<float> *)tw, (cplx<float> *)Zg, RT, scr_r);
+        kc<<<gc, thr_c, sm_c, st>>>(R, nrec_chunk, rec_begin, n_rec_total, plan, (const cplx<float> *)tw,
+                                    (const cplx<float> *)Zg, scale, win, (cplx<float> *)series, nqb, CT,
+                                    scr_c);
+    }
+    return cudaGetLastError();
 }
 
 cudaError_t launch_grid_proj(const void *snap, int precision, int N, int W, int R, int nrec_chunk,
@@ -200,13 +395,13 @@ cudaError_t launch_grid_proj(const void *snap, int precision, int N, int W, int 
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k<<<grid, threads, smem, st>>>((const double *)snap, N, R, nrec_chunk, rec_begin, n_rec_total,
                                        grid_map, plan, (const cplx<double> *)tw, scale, win,
-                                       (cplx<double> *)series, nqb, ng);
+                                       (cplx<double> *)series, nqb, ng, grid_scratch_seqs(G, ng, plan));
     } else {
         GridKernelF k = pick_kernel<float>(plan);
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k<<<grid, threads, smem, st>>>((const float *)snap, N, R, nrec_chunk, rec_begin, n_rec_total,
                                        grid_map, plan, (const cplx<float> *)tw, scale, win,
-                                       (cplx<float> *)series, nqb, ng);
+                                       (cplx<float> *)series, nqb, ng, grid_scratch_seqs(G, ng, plan));
     }
     return cudaGetLastError();
 }

@@ -93,7 +93,8 @@ struct QSet {
     int n_list = 0;
     int Q = 0;
     double list_scale = 1.0;
-    int fp64_ok = 1;           // the FP64 grid transform fits one CTA
+    int fp64_ok = 1;           // the FP64 grid transform fits (one block or two passes)
+    int large[2] = {0, 0};     // per precision (0 FP64, 1 FP32): two-pass transform
     FFTPlan gplan{};
     DevBuf tw64, tw32;        // grid twiddles
     DevBuf phase64, phase32;  // [N][n_list] complex
@@ -125,6 +126,7 @@ struct smd_ctx {
     std::map<int, std::unique_ptr<Plan>> tplans;   // keyed by n
     // job buffers (grow-only)
     DevBuf state, s0, imp, snap[2], series, qss, stats, e0, status, win, acc_tmp, in_tmp, out_tmp;
+    DevBuf gscratch;   // packed row-transformed grids of the two-pass grid transform
     int launches = 0;
     std::vector<cudaEvent_t> tev;   // timing events, reused across calls
     // bf16 high / low parts of one chunk's snapshot rows and their maps
@@ -459,9 +461,23 @@ extern "C" int smd_qset_upload(smd_ctx *ctx, int lattice_id, int use_grid, int n
     if (Q->Q <= 0) return fail(ctx, SMD_EINVAL, "qset: empty");
     if (use_grid) {
         if (!make_plan(L.G, Q->gplan, true)) return fail(ctx, SMD_EINVAL, "qset: grid size has a prime factor > 64");
-        if ((size_t)L.G * L.G > 16384) return fail(ctx, SMD_EINVAL, "qset: grid larger than 128 x 128");
-        if (!grid_proj_ng(L.G, 1, Q->gplan)) return fail(ctx, SMD_EINVAL, "qset: grid too large for the shared-memory transform");
-        if (!grid_proj_ng(L.G, 0, Q->gplan)) Q->fp64_ok = 0;
+        // SMD_GRID_TWO_PASS=1 sends grids that fit one block through the
+        // two-pass transform too (tests compare the two)
+        const char *tp = std::getenv("SMD_GRID_TWO_PASS");
+        const bool force_two = tp && std::atoi(tp) != 0;
+        for (int prec : {0, 1}) {
+            if (force_two && grid_large_ok(L.G, prec, Q->gplan)) {
+                Q->large[prec] = 1;
+                continue;
+            }
+            if (grid_proj_ng(L.G, prec, Q->gplan)) continue;
+            if (!grid_large_ok(L.G, prec, Q->gplan)) {
+                if (prec == 1) return fail(ctx, SMD_EINVAL, "qset: grid too large for the shared-memory transforms");
+                Q->fp64_ok = 0;
+            } else {
+                Q->large[prec] = 1;
+            }
+        }
         CK(upload_twiddles(L.G, Q->tw64, Q->tw32), "twiddles");
     }
     if (n_list > 0) {
@@ -831,9 +847,11 @@ int prepare(smd_ctx *ctx, const smd_job_desc *job, JobGeom &g)
     g.R = std::min(g.n_rec, 64);
     // per-sample device bytes
     const size_t N = g.N;
+    const bool large = g.Qs->use_grid && g.Qs->large[g.prec == SMD_FP64 ? 0 : 1];
     const size_t per = 2 * 3 * N * sizeof(double) + N + 2 * (size_t)g.R * 3 * N * g.elem +
                        3 * (size_t)g.n_rec * g.nqb * 16 + (size_t)g.n_rec * sizeof(double) +
-                       5 * sizeof(double);
+                       5 * sizeof(double) +
+                       (large ? grid_large_scratch(g.Qs->G, g.R, g.prec == SMD_FP64 ? 0 : 1) : 0);
     const size_t fixed = 3 * (size_t)g.Q * g.n_rec * sizeof(double) + (64u << 20);
     if (ctx->budget <= fixed + per) return fail(ctx, SMD_ENOMEM_ADMIT, "job: one sample exceeds the HBM budget");
     size_t W = (ctx->budget - fixed) / per;
@@ -937,11 +955,22 @@ int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const do
             CK(cudaEventRecord(ev(2 + 2 * nchunks + 2 * c), ctx->s_proj), "event");
             if (Qs.use_grid) {
                 const double scale = std::sqrt(1.0 / ((double)Qs.G * Qs.G));   // subrouts.cpp:8343
-                CK(launch_grid_proj(ctx->snap[b].p, g.prec, N, Ww, R, re - rb, rb, n_rec,
-                                    L.grid_map.as<int>(), Qs.gplan,
-                                    g.prec == SMD_FP64 ? Qs.tw64.p : Qs.tw32.p, scale, d_win,
-                                    ctx->series.p, nqb, ctx->s_proj), "grid projection");
-                ctx->launches++;
+                if (Qs.large[g.prec == SMD_FP64 ? 0 : 1]) {
+                    CK(ctx->gscratch.ensure((size_t)W * grid_large_scratch(Qs.G, R, g.prec == SMD_FP64 ? 0 : 1)),
+                       "cudaMalloc grid scratch");
+                    CK(launch_grid_proj_large(ctx->snap[b].p, g.prec, N, Ww, R, re - rb, rb, n_rec,
+                                              L.grid_map.as<int>(), Qs.gplan,
+                                              g.prec == SMD_FP64 ? Qs.tw64.p : Qs.tw32.p, scale, d_win,
+                                              ctx->series.p, nqb, ctx->gscratch.p, ctx->s_proj),
+                       "grid projection (two passes)");
+                    ctx->launches += 2;
+                } else {
+                    CK(launch_grid_proj(ctx->snap[b].p, g.prec, N, Ww, R, re - rb, rb, n_rec,
+                                        L.grid_map.as<int>(), Qs.gplan,
+                                        g.prec == SMD_FP64 ? Qs.tw64.p : Qs.tw32.p, scale, d_win,
+                                        ctx->series.p, nqb, ctx->s_proj), "grid projection");
+                    ctx->launches++;
+                }
             }
             if (Qs.n_list > 0 && g.prec == SMD_FP32) {
                 // split-BF16 tensor-core projection of the chunk's rows

@@ -17,6 +17,14 @@ cudaError_t launch_rk(const LatticeDev &L, const RKJob &J, int precision, bool g
 // does not fit one block
 int grid_proj_ng(int G, int precision, const FFTPlan &p);
 size_t grid_proj_smem(int G, int precision, const FFTPlan &p);
+// two-pass transform of grids too large for one block (G even, <= 512)
+bool grid_large_ok(int G, int precision, const FFTPlan &p);
+size_t grid_large_scratch(int G, int R, int precision);   // bytes per sample
+cudaError_t launch_grid_proj_large(const void *snap, int precision, int N, int W, int R,
+                                   int nrec_chunk, int rec_begin, int n_rec_total,
+                                   const int *grid_map, const FFTPlan &plan, const void *tw,
+                                   double scale, const double *win, void *series, int nqb,
+                                   void *Zg, cudaStream_t st);
 cudaError_t launch_grid_proj(const void *snap, int precision, int N, int W, int R, int nrec_chunk,
                              int rec_begin, int n_rec_total, const int *grid_map,
                              const FFTPlan &plan, const void *tw, double scale, const double *win,

@@ -103,6 +103,57 @@ def c4(n_samples: int = 512) -> Workload:
 
 WORKLOADS = {"c1": c1, "c2": c2, "c4": c4}
 
+C5_GEOMS = ("square", "triang", "hexagn", "kagome", "lieb")
+
+
+def _valid_L(geom: str, n_target: float, n_max: int) -> Optional[int]:
+    """The L whose site count is nearest n_target (log scale) among the sizes
+    the reference's lattice builders accept, N <= n_max."""
+    from .smd import geometry_info
+    from ._lib import SMDError
+    best, best_d = None, None
+    for L in range(2, 200):
+        try:
+            N = geometry_info(geom, L)[0]
+        except SMDError:
+            continue
+        if N > n_max:
+            break
+        d = abs(math.log(N / n_target))
+        if best_d is None or d < best_d:
+            best, best_d = L, d
+    return best
+
+
+def c5_stream(n_jobs: int, seed: int, n_min: int = 256, n_max: int = 4096,
+              samples=(16, 48), steps: int = 4096, stride: int = 4):
+    """Jobs of the serving workload: lattice drawn uniformly from the five
+    crystal types, N log-uniform in [n_min, n_max] snapped to a valid L,
+    J1 = 1, J2 in [0, 0.8], JX in [0, 0.2], lambda in [0.8, 1.0], h in
+    [0, 0.5], 0-10 % vacancies, seeded ordered states with Gaussian tilts,
+    grid q, FP32 form.  (The full configuration reaches N = 16384, 256
+    samples and 2^15 steps; bench.py bounds N, samples and steps so the
+    stream fits a few seconds.)  Returns [(Workload, imp ratio)]."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    states = {"square": "stripe", "triang": "q120"}
+    while len(jobs) < n_jobs:
+        geom = C5_GEOMS[rng.integers(len(C5_GEOMS))]
+        L = _valid_L(geom, math.exp(rng.uniform(math.log(n_min), math.log(n_max))), n_max)
+        if L is None:
+            continue
+        lam = float(rng.uniform(0.8, 1.0))
+        s = SMDSettings(geom=geom, L=L, J1=1.0, J2=float(rng.uniform(0.0, 0.8)),
+                        JX=float(rng.uniform(0.0, 0.2)), zlamb1=lam, zlamb2=lam,
+                        h=float(rng.uniform(0.0, 0.5)), imp_ratio=float(rng.uniform(0.0, 0.1)),
+                        dtm=0.01, ntm=steps // stride)
+        n = int(rng.integers(samples[0], samples[1] + 1))
+        s = dataclasses.replace(s, NMeas=1000 * n)
+        w = Workload(f"c5_{len(jobs)}", s, n, states.get(geom, "ferro"), 0.1, stride,
+                     steps // stride, SMD_FP32, 16, 0, seed + 101 * len(jobs))
+        jobs.append(w)
+    return jobs
+
 
 def make_inputs(w: Workload, rank: int = 0):
     """Samples (and per-sample impurity maps) for one rank."""

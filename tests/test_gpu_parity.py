@@ -125,6 +125,49 @@ def test_time_transform_lengths_vs_oracle(ctx, oracle_mod, precision, n_rec):
             assert np.linalg.norm(a - b) / np.linalg.norm(b) <= 1e-3
 
 
+@pytest.mark.parametrize("geom,L", [("kagome", 12), ("hexagn", 6), ("square", 16)])
+def test_two_pass_grid_transform_vs_oracle(ctx, oracle_mod, monkeypatch, geom, L):
+    """The two-pass grid transform (rows, then columns through a global
+    scratch) against the oracle, FP64, on grids that also fit one block."""
+    monkeypatch.setenv("SMD_GRID_TWO_PASS", "1")
+    s = SMDSettings(geom=geom, L=L, J2=0.3, JX=0.05, dtm=0.01, ntm=24, window="hann1")
+    lat, lid = _upload(ctx, s)
+    qid = ctx.qset(lid, use_grid=True)
+    kind = "stripe" if geom == "square" else "ferro"
+    spins, _ = smp.make_samples(s, 3, kind, 0.4, 12)
+    win = smd.window("hann1", 24)
+    r = ctx.run(lid, qid, spins, s.dtm, 24, stride=2, win=win)
+    m = oracle_mod.Model(s, oracle_mod.make_lattice(geom, L))
+    acc = 0.0
+    for k in range(3):
+        acc = acc + oracle_mod.dyn_spectrum(m, spins[k], s.dtm, 24, stride=2, win=win)["spec"]
+    acc /= 3
+    assert np.max(np.abs(r.spec - acc)) <= SPEC_TOL * np.max(np.abs(acc))
+
+
+@pytest.mark.parametrize("precision", [_lib.SMD_FP64, _lib.SMD_FP32])
+def test_grid_larger_than_one_block(ctx, oracle_mod, precision):
+    """Honeycomb L = 48 (N = 4608, a 144 x 144 grid, beyond one block): the
+    two-pass transform against the oracle (FP64 within 1e-10, FP32 form
+    within 1e-3 rel-L2)."""
+    s = SMDSettings(geom="hexagn", L=48, J2=0.2, dtm=0.01, ntm=16, window="hann1")
+    lat, lid = _upload(ctx, s)
+    qid = ctx.qset(lid, use_grid=True)
+    spins, _ = smp.make_samples(s, 2, "ferro", 0.3, 21)
+    win = smd.window("hann1", 16)
+    kw = dict(precision=precision, fix_every=16) if precision == _lib.SMD_FP32 else {}
+    r = ctx.run(lid, qid, spins, s.dtm, 16, win=win, **kw)
+    m = oracle_mod.Model(s, oracle_mod.make_lattice("hexagn", 48))
+    acc = 0.0
+    for k in range(2):
+        acc = acc + oracle_mod.dyn_spectrum(m, spins[k], s.dtm, 16, win=win)["spec"]
+    acc /= 2
+    if precision == _lib.SMD_FP64:
+        assert np.max(np.abs(r.spec - acc)) <= SPEC_TOL * np.max(np.abs(acc))
+    else:
+        assert np.linalg.norm(r.spec - acc) / np.linalg.norm(acc) <= 1e-3
+
+
 def test_list_points_on_the_grid_equal_grid_values(ctx):
     s = SMDSettings(geom="kagome", L=6, J2=0.3, dtm=0.01, ntm=16)
     lat, lid = _upload(ctx, s)
