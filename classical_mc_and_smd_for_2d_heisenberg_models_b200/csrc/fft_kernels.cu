@@ -591,12 +591,12 @@ cudaError_t launch_time_fft(const void *series, int precision, int W, int Q, int
         const int ntile = (nqb * qb + nseq - 1) / nseq;
         if (precision == 0) {
             auto k = time_fft_pow2_kernel<double>;
-            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            allow_dynamic_smem(k);
             k<<<3 * ntile, threads, smem, st>>>((const cplx<double> *)series, W, Q, nqb, n, l2, nseq,
                                                 (const cplx<double> *)tw, acc, status);
         } else {
             auto k = time_fft_pow2_kernel<float>;
-            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            allow_dynamic_smem(k);
             k<<<3 * ntile, threads, smem, st>>>((const cplx<float> *)series, W, Q, nqb, n, l2, nseq,
                                                 (const cplx<float> *)tw, acc, status);
         }
@@ -609,12 +609,12 @@ cudaError_t launch_time_fft(const void *series, int precision, int W, int Q, int
     const int fl = fft_plan_flags(plan), gen = (fl & FK_GEN) ? 1 : 0;
     if (precision == 0) {
         auto k = time_kernel<double>(fl);
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        allow_dynamic_smem(k);
         k<<<3 * ntile, threads, smem, st>>>((const cplx<double> *)series, W, Q, nqb, qt, plan,
                                             (const cplx<double> *)tw, acc, gen);
     } else {
         auto k = time_kernel<float>(fl);
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        allow_dynamic_smem(k);
         k<<<3 * ntile, threads, smem, st>>>((const cplx<float> *)series, W, Q, nqb, qt, plan,
                                             (const cplx<float> *)tw, acc, gen);
     }

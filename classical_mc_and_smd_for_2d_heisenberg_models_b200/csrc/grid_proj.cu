@@ -357,8 +357,8 @@ cudaError_t launch_grid_proj_large(const void *snap, int precision, int N, int W
         auto kr = gen ? grid_rows_kernel<double, double, FK_R16 | FK_R3 | FK_GEN>
                       : grid_rows_kernel<double, double, FK_R16 | FK_R3>;
         auto kc = gen ? grid_cols_kernel<double, FK_R16 | FK_R3 | FK_GEN> : grid_cols_kernel<double, FK_R16 | FK_R3>;
-        cudaFuncSetAttribute(kr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_r);
-        cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_c);
+        allow_dynamic_smem(kr);
+        allow_dynamic_smem(kc);
         kr<<<gr, thr_r, sm_r, st>>>((const double *)snap, N, R, nrec_chunk, grid_map, plan,
                                     (const cplx<double> *)tw, (cplx<double> *)Zg, RT, scr_r);
         kc<<<gc, thr_c, sm_c, st>>>(R, nrec_chunk, rec_begin, n_rec_total, plan, (const cplx<double> *)tw,
@@ -368,8 +368,8 @@ cudaError_t launch_grid_proj_large(const void *snap, int precision, int N, int W
         auto kr = gen ? grid_rows_kernel<float, float, FK_R16 | FK_R3 | FK_GEN>
                       : grid_rows_kernel<float, float, FK_R16 | FK_R3>;
         auto kc = gen ? grid_cols_kernel<float, FK_R16 | FK_R3 | FK_GEN> : grid_cols_kernel<float, FK_R16 | FK_R3>;
-        cudaFuncSetAttribute(kr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_r);
-        cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_c);
+        allow_dynamic_smem(kr);
+        allow_dynamic_smem(kc);
         kr<<<gr, thr_r, sm_r, st>>>((const float *)snap, N, R, nrec_chunk, grid_map, plan,
                                     (const cplx<float> *)tw, (cplx<float> *)Zg, RT, scr_r);
         kc<<<gc, thr_c, sm_c, st>>>(R, nrec_chunk, rec_begin, n_rec_total, plan, (const cplx<float> *)tw,
@@ -392,13 +392,13 @@ cudaError_t launch_grid_proj(const void *snap, int precision, int N, int W, int 
     dim3 grid(((nrec_chunk + 1) / 2) * (3 / ng), W);
     if (precision == 0) {
         GridKernelD k = pick_kernel<double>(plan);
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        allow_dynamic_smem(k);
         k<<<grid, threads, smem, st>>>((const double *)snap, N, R, nrec_chunk, rec_begin, n_rec_total,
                                        grid_map, plan, (const cplx<double> *)tw, scale, win,
                                        (cplx<double> *)series, nqb, ng, grid_scratch_seqs(G, ng, plan));
     } else {
         GridKernelF k = pick_kernel<float>(plan);
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        allow_dynamic_smem(k);
         k<<<grid, threads, smem, st>>>((const float *)snap, N, R, nrec_chunk, rec_begin, n_rec_total,
                                        grid_map, plan, (const cplx<float> *)tw, scale, win,
                                        (cplx<float> *)series, nqb, ng, grid_scratch_seqs(G, ng, plan));

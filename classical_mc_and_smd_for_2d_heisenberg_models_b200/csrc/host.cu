@@ -32,6 +32,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <set>
 #include <string>
 #include <tuple>
@@ -57,6 +58,9 @@ struct DevBuf {
     {
         if (b <= bytes) return cudaSuccess;
         release();
+        // below 1 GB, a quarter of headroom: a stream of growing jobs then
+        // reallocates (and synchronises the device) rarely
+        if (b < ((size_t)1 << 30)) b = (b + b / 4 + ((size_t)2 << 20) - 1) & ~(((size_t)2 << 20) - 1);
         cudaError_t e = cudaMalloc(&p, b);
         if (e == cudaSuccess) bytes = b;
         else p = nullptr;
@@ -81,6 +85,7 @@ struct Lattice {
     std::vector<double> pos;
     std::vector<int> nbr_h[3];      // host copies of the active shells' tables
     std::map<int, std::unique_ptr<ClusterTab>> ctabs;   // keyed by CTAs per sample
+    std::mutex cache_mu;            // guards ctabs and the row-band fields
     // row-band kernel: stencil geometry (-2 unchecked, -1 not applicable),
     // cells per side, active shells
     int rows_geom = -2, side = 0, rows_shells = 0;
@@ -121,8 +126,11 @@ struct smd_ctx {
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     std::string err;
     int next_id = 1;
-    std::map<int, std::unique_ptr<Lattice>> lattices;
-    std::map<int, std::unique_ptr<QSet>> qsets;
+    // lattices and q sets are shared with the serving lanes' contexts
+    // (smd_share_objects); maps_mu guards the maps
+    std::mutex maps_mu;
+    std::map<int, std::shared_ptr<Lattice>> lattices;
+    std::map<int, std::shared_ptr<QSet>> qsets;
     std::map<int, std::unique_ptr<Plan>> tplans;   // keyed by n
     // job buffers (grow-only)
     DevBuf state, s0, imp, snap[2], series, qss, stats, e0, status, win, acc_tmp, in_tmp, out_tmp;
@@ -426,7 +434,10 @@ extern "C" int smd_lattice_upload(smd_ctx *ctx, const smd_lattice_desc *d, int *
             L->nbr_h[s].assign(d->nbr[s], d->nbr[s] + (size_t)N * d->zn[s]);
     }
     const int id = ctx->next_id++;
-    ctx->lattices[id] = std::move(L);
+    {
+        std::lock_guard<std::mutex> lk(ctx->maps_mu);
+        ctx->lattices[id] = std::move(L);
+    }
     *lattice_id = id;
     return SMD_OK;
 }
@@ -436,6 +447,7 @@ extern "C" int smd_lattice_free(smd_ctx *ctx, int lattice_id)
     if (!ctx) return SMD_EINVAL;
     cudaSetDevice(ctx->device);
     cudaDeviceSynchronize();
+    std::lock_guard<std::mutex> lk(ctx->maps_mu);
     if (!ctx->lattices.erase(lattice_id)) return SMD_ENOTFOUND;
     return SMD_OK;
 }
@@ -444,9 +456,14 @@ extern "C" int smd_qset_upload(smd_ctx *ctx, int lattice_id, int use_grid, int n
                                const double *qlist, double list_scale, int *qset_id)
 {
     if (!ctx || !qset_id) return SMD_EINVAL;
-    auto it = ctx->lattices.find(lattice_id);
-    if (it == ctx->lattices.end()) return fail(ctx, SMD_ENOTFOUND, "qset: unknown lattice");
-    Lattice &L = *it->second;
+    std::shared_ptr<Lattice> Lp;
+    {
+        std::lock_guard<std::mutex> lk(ctx->maps_mu);
+        auto it = ctx->lattices.find(lattice_id);
+        if (it == ctx->lattices.end()) return fail(ctx, SMD_ENOTFOUND, "qset: unknown lattice");
+        Lp = it->second;
+    }
+    Lattice &L = *Lp;
     if (n_list < 0 || (n_list > 0 && !qlist)) return fail(ctx, SMD_EINVAL, "qset: bad q list");
     if (n_list > 0 && L.pos.empty()) return fail(ctx, SMD_EINVAL, "qset: lattice has no positions");
     if (use_grid && L.G <= 0) return fail(ctx, SMD_EINVAL, "qset: lattice has no DFT grid");
@@ -516,7 +533,10 @@ extern "C" int smd_qset_upload(smd_ctx *ctx, int lattice_id, int use_grid, int n
             return fail(ctx, SMD_ECUDA, "qset: tensor map encoding failed");
     }
     const int id = ctx->next_id++;
-    ctx->qsets[id] = std::move(Q);
+    {
+        std::lock_guard<std::mutex> lk(ctx->maps_mu);
+        ctx->qsets[id] = std::move(Q);
+    }
     *qset_id = id;
     return SMD_OK;
 }
@@ -524,6 +544,7 @@ extern "C" int smd_qset_upload(smd_ctx *ctx, int lattice_id, int use_grid, int n
 extern "C" int smd_qset_size(smd_ctx *ctx, int qset_id, int *Q)
 {
     if (!ctx || !Q) return SMD_EINVAL;
+    std::lock_guard<std::mutex> lk(ctx->maps_mu);
     auto it = ctx->qsets.find(qset_id);
     if (it == ctx->qsets.end()) return SMD_ENOTFOUND;
     *Q = it->second->Q;
@@ -549,6 +570,7 @@ struct JobGeom {
 // does not fit the cluster kernel's limits.
 ClusterTab *cluster_tables(Lattice &L, int CS)
 {
+    std::lock_guard<std::mutex> lk(L.cache_mu);
     auto it = L.ctabs.find(CS);
     if (it != L.ctabs.end()) return it->second.get();
     const int N = L.N;
@@ -680,6 +702,7 @@ ClusterTab *cluster_tables(Lattice &L, int CS)
 // triangular stencil.
 void rows_check(Lattice &L)
 {
+    std::lock_guard<std::mutex> lk(L.cache_mu);
     if (L.rows_geom != -2) return;
     L.rows_geom = -1;
     const int N = L.N;
@@ -806,10 +829,12 @@ void choose_cluster(smd_ctx *ctx, JobGeom &g, int n_samples)
 int prepare(smd_ctx *ctx, const smd_job_desc *job, JobGeom &g)
 {
     if (!job) return fail(ctx, SMD_EINVAL, "job: null");
+    std::unique_lock<std::mutex> mlk(ctx->maps_mu);
     auto li = ctx->lattices.find(job->lattice);
     if (li == ctx->lattices.end()) return fail(ctx, SMD_ENOTFOUND, "job: unknown lattice");
     auto qi = ctx->qsets.find(job->qset);
     if (qi == ctx->qsets.end()) return fail(ctx, SMD_ENOTFOUND, "job: unknown q set");
+    mlk.unlock();
     if (qi->second->lattice != job->lattice) return fail(ctx, SMD_EINVAL, "job: q set belongs to another lattice");
     if (job->n_samples < 1) return fail(ctx, SMD_EINVAL, "job: n_samples < 1");
     if (job->n_rec < 2) return fail(ctx, SMD_EINVAL, "job: n_rec < 2");
@@ -1149,9 +1174,10 @@ extern "C" int smd_dyn_spectrum_ref(smd_ctx *ctx, int lattice_id, int qset_id, d
     int rc = smd_qset_size(ctx, qset_id, &Q);
     if (rc) return rc;
     std::vector<double> spec((size_t)3 * Q * ntm), fin;
-    auto li = ctx->lattices.find(lattice_id);
-    if (li == ctx->lattices.end()) return SMD_ENOTFOUND;
-    fin.resize((size_t)li->second->N * 3);
+    int N = 0;
+    rc = smd_lattice_sites(ctx, lattice_id, &N);
+    if (rc) return rc;
+    fin.resize((size_t)N * 3);
     rc = smd_run(ctx, &job, spinField, tWinVec, spec.data(), qSStVec, fin.data(), nullptr);
     if (rc) return rc;
     const size_t blk = (size_t)Q * ntm;
@@ -1166,13 +1192,18 @@ extern "C" int smd_evolve(smd_ctx *ctx, int lattice_id, int precision, int n_sam
                           int nsteps, int fix_every, const int *imp, double *spins, smd_report *rep)
 {
     if (!ctx || !spins || nsteps < 1) return SMD_EINVAL;
-    auto li = ctx->lattices.find(lattice_id);
-    if (li == ctx->lattices.end()) return fail(ctx, SMD_ENOTFOUND, "evolve: unknown lattice");
+    std::shared_ptr<Lattice> Lp;
+    {
+        std::lock_guard<std::mutex> lk(ctx->maps_mu);
+        auto li = ctx->lattices.find(lattice_id);
+        if (li == ctx->lattices.end()) return fail(ctx, SMD_ENOTFOUND, "evolve: unknown lattice");
+        Lp = li->second;
+    }
     // a q set of one list point keeps the pipeline shape; two records
     // (start and end) with stride nsteps give the final state
     int qid = -1;
     double q0[2] = {0.0, 0.0};
-    Lattice &L = *li->second;
+    Lattice &L = *Lp;
     std::vector<double> fake_pos;
     if (L.pos.empty()) L.pos.assign(2 * (size_t)L.N, 0.0);
     int rc = smd_qset_upload(ctx, lattice_id, 0, 1, q0, 1.0, &qid);
@@ -1190,7 +1221,10 @@ extern "C" int smd_evolve(smd_ctx *ctx, int lattice_id, int precision, int n_sam
     std::vector<double> spec(3 * 2), qss(2), win(2, 1.0);
     if (precision == SMD_FP32) {
         // the FP32 form has no list projection yet; use the grid if present
-        ctx->qsets.erase(qid);
+        {
+            std::lock_guard<std::mutex> lk(ctx->maps_mu);
+            ctx->qsets.erase(qid);
+        }
         rc = smd_qset_upload(ctx, lattice_id, 1, 0, nullptr, 1.0, &qid);
         if (rc) return rc;
         int Q = 0;
@@ -1199,16 +1233,50 @@ extern "C" int smd_evolve(smd_ctx *ctx, int lattice_id, int precision, int n_sam
         job.qset = qid;
     }
     rc = smd_run(ctx, &job, spins, win.data(), spec.data(), qss.data(), spins, rep);
-    ctx->qsets.erase(qid);
+    {
+        std::lock_guard<std::mutex> lk(ctx->maps_mu);
+        ctx->qsets.erase(qid);
+    }
     return rc;
 }
 
 // ------------------------------------------------------------- serving
+
+// Internal (not exported): serving lanes run jobs on contexts of their own
+// (streams and working buffers), sharing the parent's lattice and q set.
+int smd_share_objects(smd_ctx *from, smd_ctx *to, int lattice_id, int qset_id)
+{
+    std::shared_ptr<Lattice> L;
+    std::shared_ptr<QSet> Q;
+    {
+        std::lock_guard<std::mutex> lk(from->maps_mu);
+        auto li = from->lattices.find(lattice_id);
+        auto qi = from->qsets.find(qset_id);
+        if (li == from->lattices.end() || qi == from->qsets.end()) return SMD_ENOTFOUND;
+        L = li->second;
+        Q = qi->second;
+    }
+    std::lock_guard<std::mutex> lk(to->maps_mu);
+    to->lattices[lattice_id] = L;
+    to->qsets[qset_id] = Q;
+    return SMD_OK;
+}
+
+int smd_ctx_device(const smd_ctx *ctx) { return ctx->device; }
+
+// a lane's failure, reported through the parent's smd_last_error
+void smd_copy_error(smd_ctx *to, const smd_ctx *from, long long job_id)
+{
+    std::lock_guard<std::mutex> lk(to->maps_mu);
+    to->err = "job " + std::to_string(job_id) + ": " + from->err;
+}
+size_t smd_ctx_budget(const smd_ctx *ctx) { return ctx->budget; }
 // (smd_submit and the rest: serve.cpp)
 
 extern "C" int smd_lattice_sites(smd_ctx *ctx, int lattice_id, int *N)
 {
     if (!ctx || !N) return SMD_EINVAL;
+    std::lock_guard<std::mutex> lk(ctx->maps_mu);
     auto it = ctx->lattices.find(lattice_id);
     if (it == ctx->lattices.end()) return SMD_ENOTFOUND;
     *N = it->second->N;

@@ -346,7 +346,7 @@ cudaError_t launch_list_proj_tc(const CUtensorMap &Ah, const CUtensorMap &Al, co
                                 void *series, int nqb, int qoff, int *status, cudaStream_t st)
 {
     auto k = tc::list_proj_tc_kernel;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM);
+    cudaError_t e = allow_dynamic_smem(k);
     if (e != cudaSuccess) return e;
     dim3 grid((2 * Lq + tc::BN - 1) / tc::BN, (M + tc::BM - 1) / tc::BM);
     k<<<grid, 128, tc::SMEM, st>>>(Ah, Al, Bh, Bl, M, kp / tc::BK, R, nrec_chunk, rec_begin,

@@ -591,7 +591,7 @@ cudaError_t launch_cluster_t(const ClusterParams &P, const RKJob &J, int threads
                              cudaStream_t st)
 {
     auto k = rk_cluster_kernel<T, SPT, ZT>;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = allow_dynamic_smem(k);
     if (e != cudaSuccess) return e;
     if (P.CS > 8) {
         e = cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);

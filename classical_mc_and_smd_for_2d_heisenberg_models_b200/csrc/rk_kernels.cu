@@ -764,12 +764,12 @@ static cudaError_t launch_one(const LatticeDev &L, const RKJob &J, int precision
 {
     if (precision == 0) {
         auto k = rk_fp64_kernel<MAXSPT, GEN>;
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = allow_dynamic_smem(k);
         if (e != cudaSuccess) return e;
         k<<<J.n_samples, threads, smem, st>>>(L, J);
     } else {
         auto k = rk_fp32_kernel<MAXSPT, GEN>;
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = allow_dynamic_smem(k);
         if (e != cudaSuccess) return e;
         k<<<J.n_samples, threads, smem, st>>>(L, J);
     }

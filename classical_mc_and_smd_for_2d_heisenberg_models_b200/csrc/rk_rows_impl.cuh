@@ -617,7 +617,7 @@ cudaError_t launch_rows_t(const RowsParams &P, const RKJob &J, int threads, size
 {
     constexpr int SPT = rows_spt(sizeof(T) == 8 ? 0 : 1);
     auto k = rk_rows_kernel<T, SPT, GEOM, SH>;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = allow_dynamic_smem(k);
     if (e != cudaSuccess) return e;
     if (P.CS > 8) {
         e = cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);

@@ -1,13 +1,24 @@
 // serve.cpp -- job submission interface (smd_submit / smd_poll / smd_wait /
 // smd_cancel).
 //
-// Jobs are copied at submit time and executed by one worker thread per
-// context, in arrival order, through smd_run.  The output buffers named at
-// submit are written when the job finishes; smd_poll reports SMD_EBUSY until
-// then and returns the job's latency (submit to completion) afterwards.
+// Jobs are copied at submit time and taken in arrival order by K worker
+// lanes per context (SMD_SERVE_LANES, default 1).  Each lane owns a context
+// of its own -- streams, working buffers and an equal share of the HBM
+// budget, which admits its jobs -- and shares the parent's lattices and q
+// sets, so up to K jobs run on the device at once and small jobs, which
+// leave SMs idle on their own, overlap.  On the serving mix of the bench
+// (jobs of 256-4096 sites whose RK launches already fill the SMs) four
+// lanes measured slower than one (p50 70 vs 56 ms), so one is the default.
+// A job's result is that of smd_run of the job alone.  The output buffers named at submit are written when
+// the job finishes; smd_poll reports SMD_EBUSY until then and returns the
+// job's latency (submit to completion) afterwards.
 #include "../../include/smd_b200.h"
 
+#include <cuda_runtime.h>
+
+#include <algorithm>
 #include <chrono>
+#include <cstdlib>
 #include <condition_variable>
 #include <deque>
 #include <map>
@@ -15,6 +26,12 @@
 #include <mutex>
 #include <thread>
 #include <vector>
+
+// host.cu internals shared with the lanes
+int smd_share_objects(smd_ctx *from, smd_ctx *to, int lattice_id, int qset_id);
+int smd_ctx_device(const smd_ctx *ctx);
+size_t smd_ctx_budget(const smd_ctx *ctx);
+void smd_copy_error(smd_ctx *to, const smd_ctx *from, long long job_id);
 
 namespace {
 
@@ -37,16 +54,25 @@ struct Server {
     std::map<long long, std::shared_ptr<Job>> jobs;
     long long next = 1;
     bool stop = false;
-    std::thread worker;
+    std::vector<std::thread> workers;
 
-    void run()
+    void run(int lanes)
     {
+        // the lane's own context
+        smd_ctx *w = nullptr;
+        smd_device_opts o{};
+        o.device = smd_ctx_device(ctx);
+        size_t fr = 0, tot = 0;
+        cudaSetDevice(o.device);
+        cudaMemGetInfo(&fr, &tot);
+        o.hbm_budget = std::min(smd_ctx_budget(ctx), (size_t)(0.85 * (double)fr)) / (size_t)lanes;
+        const int crc = smd_ctx_create(&o, &w);
         for (;;) {
             std::shared_ptr<Job> j;
             {
                 std::unique_lock<std::mutex> lk(mu);
                 cv.wait(lk, [&] { return stop || !queue.empty(); });
-                if (stop && queue.empty()) return;
+                if (stop && queue.empty()) break;
                 j = queue.front();
                 queue.pop_front();
                 if (j->cancelled) {
@@ -57,8 +83,11 @@ struct Server {
                 }
             }
             j->desc.imp = j->imp.empty() ? nullptr : j->imp.data();
-            const int rc = smd_run(ctx, &j->desc, j->spins.data(), j->window.data(), j->spec_out,
-                                   j->qss_out, nullptr, nullptr);
+            int rc = crc ? SMD_ECUDA : smd_share_objects(ctx, w, j->desc.lattice, j->desc.qset);
+            if (rc == SMD_OK)
+                rc = smd_run(w, &j->desc, j->spins.data(), j->window.data(), j->spec_out,
+                             j->qss_out, nullptr, nullptr);
+            if (rc != SMD_OK && w) smd_copy_error(ctx, w, j->id);   // for smd_last_error
             {
                 std::lock_guard<std::mutex> lk(mu);
                 j->status = rc;
@@ -66,11 +95,14 @@ struct Server {
             }
             done_cv.notify_all();
         }
+        if (w) smd_ctx_destroy(w);
     }
 };
 
 std::mutex g_mu;
-std::map<smd_ctx *, std::unique_ptr<Server>> g_servers;
+// never destroyed: lanes still blocked at process exit must not meet a
+// destroyed registry (smd_serve_shutdown is the orderly end)
+auto &g_servers = *new std::map<smd_ctx *, std::unique_ptr<Server>>();
 
 Server *server_for(smd_ctx *ctx)
 {
@@ -80,7 +112,10 @@ Server *server_for(smd_ctx *ctx)
     auto s = std::make_unique<Server>();
     s->ctx = ctx;
     Server *p = s.get();
-    p->worker = std::thread([p] { p->run(); });
+    int lanes = 1;
+    if (const char *e = std::getenv("SMD_SERVE_LANES")) lanes = std::atoi(e);
+    lanes = std::max(1, std::min(lanes, 16));
+    for (int i = 0; i < lanes; i++) p->workers.emplace_back([p, lanes] { p->run(lanes); });
     g_servers[ctx] = std::move(s);
     return p;
 }
@@ -102,7 +137,8 @@ extern "C" void smd_serve_shutdown(smd_ctx *ctx)
         s->stop = true;
     }
     s->cv.notify_all();
-    if (s->worker.joinable()) s->worker.join();
+    for (auto &t : s->workers)
+        if (t.joinable()) t.join();
 }
 
 extern "C" int smd_submit(smd_ctx *ctx, const smd_job_desc *job, const double *spins0,

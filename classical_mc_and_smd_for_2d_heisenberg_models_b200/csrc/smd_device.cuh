@@ -65,6 +65,28 @@ struct FFTPlan {
     int radix[16];
 };
 
+// Dynamic shared memory of a kernel: the limit is process-wide per kernel,
+// so every launcher sets it to the device's opt-in maximum less the
+// kernel's static shared memory (one value from every thread) instead of to
+// its own launch's size, which a concurrent launch from another thread (the
+// serving lanes) could undercut.
+template <typename K>
+inline cudaError_t allow_dynamic_smem(K kernel)
+{
+    static int max_optin = 0;
+    if (!max_optin) {
+        int dev = 0, mx = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&mx, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        max_optin = mx;
+    }
+    cudaFuncAttributes fa{};
+    cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                max_optin - (int)fa.sharedSizeBytes);
+}
+
 template <typename T>
 struct cplx {
     T x, y;

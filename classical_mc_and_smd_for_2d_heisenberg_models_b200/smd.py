@@ -312,7 +312,7 @@ class Context:
         lat = C.c_double()
         rc = self.lib.smd_wait(self.h, job_id, timeout_ms, C.byref(lat))
         if rc:
-            raise SMDError(rc, f"job {job_id}")
+            raise SMDError(rc, f"job {job_id} ({self.lib.smd_last_error(self.h).decode()})")
         spec, qss = self._keep.pop(("job", job_id))
         return spec, qss, lat.value
 

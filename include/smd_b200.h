@@ -206,10 +206,12 @@ SMD_API int smd_evolve(smd_ctx *ctx, int lattice_id, int precision, int n_sample
 
 /* ------------------------------------------------------------- serving */
 
-/* Job queue: a submitted job is copied, then run by the context's worker
- * thread in arrival order, each job as smd_run of the job alone (its waves
- * sized by the HBM budget).  Outputs go to the host buffers given at
- * submit, valid once smd_poll returns SMD_OK. */
+/* Job queue: a submitted job is copied, then taken in arrival order by one
+ * of the context's worker lanes (SMD_SERVE_LANES, default 1), each with its
+ * own streams, buffers and an equal share of the HBM budget, so with more
+ * than one lane several jobs run on the device at once; each job's result
+ * is that of smd_run of the job alone.  Outputs go to the host buffers given at submit, valid
+ * once smd_poll returns SMD_OK. */
 SMD_API int smd_submit(smd_ctx *ctx, const smd_job_desc *job, const double *spins0,
                const double *window, double *spec_out, double *qss_out,
                long long *job_id);
