@@ -138,10 +138,11 @@ struct smd_ctx {
     int launches = 0;
     std::vector<cudaEvent_t> tev;   // timing events, reused across calls
     // bf16 high / low parts of one chunk's snapshot rows and their maps
-    DevBuf ahi, alo;
-    CUtensorMap map_ahi{}, map_alo{};
-    const void *map_a_base = nullptr;
-    int map_a_rows = 0, map_a_kp = 0;
+    // split-BF16 snapshot rows, one pair per snapshot buffer
+    DevBuf ahi[2], alo[2];
+    CUtensorMap map_ahi[2]{}, map_alo[2]{};
+    const void *map_a_base[2] = {nullptr, nullptr};
+    int map_a_rows[2] = {0, 0}, map_a_kp[2] = {0, 0};
 };
 
 namespace {
@@ -965,6 +966,31 @@ int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const do
             J.qss = ctx->qss.as<double>();
             J.stats = ctx->stats.as<double>();
             J.status = ctx->status.as<int>();
+            // the cluster kernel writes the tensor-core operand rows itself
+            const bool tc_list = Qs.n_list > 0 && g.prec == SMD_FP32;
+            const bool fused_split = tc_list && g.ctab && !g.rows;
+            if (tc_list) {
+                const int rows = Ww * R * 3, kp = Qs.kp;
+                const size_t ab = (size_t)W * R * 3 * kp * 2;
+                for (DevBuf *d : {&ctx->ahi[b], &ctx->alo[b]}) {
+                    const void *old = d->p;
+                    CK(d->ensure(ab), "cudaMalloc");
+                    if (d->p != old)   // fresh rows: the padding columns past N stay zero
+                        CK(cudaMemsetAsync(d->p, 0, d->bytes, ctx->s_rk), "memset");
+                }
+                if (ctx->map_a_base[b] != ctx->ahi[b].p || ctx->map_a_rows[b] != rows ||
+                    ctx->map_a_kp[b] != kp) {
+                    if (!make_bf16_map(&ctx->map_ahi[b], ctx->ahi[b].p, rows, kp, tc_bm()) ||
+                        !make_bf16_map(&ctx->map_alo[b], ctx->alo[b].p, rows, kp, tc_bm()))
+                        return fail(ctx, SMD_ECUDA, "tensor map encoding failed");
+                    ctx->map_a_base[b] = ctx->ahi[b].p;
+                    ctx->map_a_rows[b] = rows;
+                    ctx->map_a_kp[b] = kp;
+                }
+            }
+            J.bf_hi = fused_split ? ctx->ahi[b].p : nullptr;
+            J.bf_lo = fused_split ? ctx->alo[b].p : nullptr;
+            J.bf_kp = Qs.kp;
             CK(cudaEventRecord(ev(2 + 2 * c), ctx->s_rk), "event");
             if (g.rows)
                 CK(launch_rk_rows(g.rp, J, g.prec, ctx->s_rk), "rk row-band kernel");
@@ -997,26 +1023,19 @@ int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const do
                     ctx->launches++;
                 }
             }
-            if (Qs.n_list > 0 && g.prec == SMD_FP32) {
+            if (tc_list) {
                 // split-BF16 tensor-core projection of the chunk's rows
                 const int rows = Ww * R * 3, kp = Qs.kp;
-                CK(ctx->ahi.ensure((size_t)W * R * 3 * kp * 2), "cudaMalloc");
-                CK(ctx->alo.ensure((size_t)W * R * 3 * kp * 2), "cudaMalloc");
-                if (ctx->map_a_base != ctx->ahi.p || ctx->map_a_rows != rows || ctx->map_a_kp != kp) {
-                    if (!make_bf16_map(&ctx->map_ahi, ctx->ahi.p, rows, kp, tc_bm()) ||
-                        !make_bf16_map(&ctx->map_alo, ctx->alo.p, rows, kp, tc_bm()))
-                        return fail(ctx, SMD_ECUDA, "tensor map encoding failed");
-                    ctx->map_a_base = ctx->ahi.p;
-                    ctx->map_a_rows = rows;
-                    ctx->map_a_kp = kp;
+                if (!fused_split) {
+                    CK(launch_split_bf16(ctx->snap[b].as<float>(), rows, N, kp, ctx->ahi[b].p,
+                                         ctx->alo[b].p, ctx->s_proj), "bf16 split");
+                    ctx->launches++;
                 }
-                CK(launch_split_bf16(ctx->snap[b].as<float>(), rows, N, kp, ctx->ahi.p, ctx->alo.p,
-                                     ctx->s_proj), "bf16 split");
-                CK(launch_list_proj_tc(ctx->map_ahi, ctx->map_alo, Qs.map_bhi, Qs.map_blo, rows, kp,
-                                       R, re - rb, rb, n_rec, Qs.n_list, d_win, ctx->series.p, nqb,
+                CK(launch_list_proj_tc(ctx->map_ahi[b], ctx->map_alo[b], Qs.map_bhi, Qs.map_blo, rows,
+                                       kp, R, re - rb, rb, n_rec, Qs.n_list, d_win, ctx->series.p, nqb,
                                        Qs.G * Qs.G, ctx->status.as<int>(), ctx->s_proj),
                    "tensor-core list projection");
-                ctx->launches += 2;
+                ctx->launches++;
             } else if (Qs.n_list > 0) {
                 CK(launch_list_proj_simt(ctx->snap[b].p, g.prec, Ww, R, re - rb, N, rb, n_rec,
                                          Qs.phase64.p, Qs.n_list, d_win, ctx->series.p, nqb, Qs.G * Qs.G,

@@ -25,6 +25,7 @@
 #pragma once
 
 #include <cooperative_groups.h>
+#include <cuda_bf16.h>
 
 #include "rk_cluster.cuh"
 
@@ -344,6 +345,17 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
                 for (int c = 0; c < 3; c++) {
                     snap[sb + (size_t)c * N + g] = (TS)S[k][c];
                     p += s0[c * N + g] * S[k][c];
+                    if constexpr (sizeof(T) == 4) {
+                        if (J.bf_hi) {
+                            // the tensor-core projection's operand rows
+                            const size_t o = ((size_t)smp * J.snap_R * 3 + (size_t)(r - J.rec_begin) * 3 + c) *
+                                                 J.bf_kp + g;
+                            const float v = (float)S[k][c];
+                            const __nv_bfloat16 h = __float2bfloat16_rn(v);
+                            reinterpret_cast<__nv_bfloat16 *>(J.bf_hi)[o] = h;
+                            reinterpret_cast<__nv_bfloat16 *>(J.bf_lo)[o] = __float2bfloat16_rn(v - __bfloat162float(h));
+                        }
+                    }
                 }
             }
         }

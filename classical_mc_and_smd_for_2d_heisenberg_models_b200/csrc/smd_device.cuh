@@ -54,6 +54,11 @@ struct RKJob {
     double *qss;             // [W][n_rec]
     double *stats;           // [W][4]: max drift, last E, E0, sigma_min
     int *status;             // nonzero after a numerical failure
+    // FP32 form with a tensor-core list projection: the record also writes
+    // the snapshot rows split into bf16 high and low parts, [W][R][3][kp]
+    // (null: a separate pass splits the snapshots)
+    void *bf_hi, *bf_lo;
+    int bf_kp;
 };
 
 enum { kStatusOK = 0, kStatusBadSigma = 1 };
