@@ -812,8 +812,11 @@ void choose_cluster(smd_ctx *ctx, JobGeom &g, int n_samples)
         ClusterTab *t = cluster_tables(L, CS);
         if (!t) continue;
         int spt = 0;
+        // sites per thread: the fewest that fit a block (SMD_RK_SPT forces one)
+        int force_spt = 0;
+        if (const char *e = std::getenv("SMD_RK_SPT")) force_spt = std::atoi(e);
         for (int s : {1, 2, 4})
-            if (s * rk_cluster_maxt(g.prec, s) >= t->P.n_own_max) {
+            if ((!force_spt || s == force_spt) && s * rk_cluster_maxt(g.prec, s) >= t->P.n_own_max) {
                 spt = s;
                 break;
             }
