@@ -633,6 +633,31 @@ ClusterTab *cluster_tables(Lattice &L, int CS)
             }
         }
     }
+    // Async halo pushes need a symmetric neighbour relation between CTAs: a
+    // site reads a halo copy owned by CTA o exactly when CTA o holds a copy
+    // of the site.  A publish's bytes also have to fit one mbarrier
+    // transaction count (below 2^20).
+    bool sym = true;
+    size_t max_halo = 0;
+    for (int r = 0; r < CS && sym; r++) {
+        max_halo = std::max(max_halo, halo[r].size());
+        std::vector<int> reads, held;
+        for (int g = base[r]; g < base[r + 1] && sym; g++) {
+            reads.clear();
+            held.clear();
+            for (int e = 0; e < zact; e++) {
+                const int j = edge(g, e);
+                if (j >= 0 && owner[j] != r) reads.push_back(owner[j]);
+            }
+            for (int c : pushes[r][g - base[r]]) held.push_back(c >> 16);
+            std::sort(reads.begin(), reads.end());
+            reads.erase(std::unique(reads.begin(), reads.end()), reads.end());
+            std::sort(held.begin(), held.end());
+            held.erase(std::unique(held.begin(), held.end()), held.end());
+            sym = reads == held;
+        }
+    }
+    const bool async_ok = sym && max_halo * 24 < (1u << 20);
     int pmax = 0;
     for (int r = 0; r < CS; r++)
         for (auto &v : pushes[r]) pmax = std::max(pmax, (int)v.size());
@@ -656,6 +681,7 @@ ClusterTab *cluster_tables(Lattice &L, int CS)
     P.pmax = pmax;
     P.ZT = ZT;
     P.energy_from_field = L.dev.energy_from_field;
+    P.async_halo = async_ok ? 1 : 0;
     P.h = L.dev.h;
     P.hf = (float)L.dev.h;
     for (int e = 0; e < kMaxEdgeSlots; e++)
@@ -997,8 +1023,13 @@ int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const do
             CK(cudaEventRecord(ev(2 + 2 * c), ctx->s_rk), "event");
             if (g.rows)
                 CK(launch_rk_rows(g.rp, J, g.prec, ctx->s_rk), "rk row-band kernel");
-            else if (g.ctab)
-                CK(launch_rk_cluster(g.ctab->P, J, g.prec, g.spt, g.threads, ctx->s_rk), "rk cluster kernel");
+            else if (g.ctab) {
+                // SMD_RK_HALO=barrier publishes halos with cluster barriers
+                ClusterParams cp = g.ctab->P;
+                if (const char *e = std::getenv("SMD_RK_HALO"))
+                    if (!std::strcmp(e, "barrier")) cp.async_halo = 0;
+                CK(launch_rk_cluster(cp, J, g.prec, g.spt, g.threads, ctx->s_rk), "rk cluster kernel");
+            }
             else
                 CK(launch_rk(L.dev, J, g.prec, gen, ctx->s_rk), "rk kernel");
             CK(cudaEventRecord(ev(3 + 2 * c), ctx->s_rk), "event");
@@ -1098,6 +1129,7 @@ int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const do
     }
     if (st & 4) return fail(ctx, SMD_ETIMEOUT, "tensor-core projection: a bounded wait expired");
     if (st & 8) return fail(ctx, SMD_ETIMEOUT, "time transform: a bounded wait expired");
+    if (st & 16) return fail(ctx, SMD_ETIMEOUT, "RK halo exchange: a bounded wait expired");
     if (st) return fail(ctx, SMD_ECUDA, "a sample reached a zero correction denominator (sigma = 0)");
     return SMD_OK;
 }

@@ -6,7 +6,11 @@
 // sites and of the halo sites (other CTAs' sites that its sites neighbour).
 // After computing a stage value a thread stores it locally and pushes it
 // into the halo slots of the CTAs that hold a copy (distributed shared
-// memory stores); one cluster barrier per stage publishes everything.
+// memory stores).  With async_halo set (the neighbour relation is
+// symmetric and a publish fits one mbarrier transaction count), the pushes
+// are st.async stores that complete bytes on one of two mbarriers of the
+// receiving CTA, and a stage waits for its own halo bytes only; otherwise
+// one cluster barrier per stage publishes everything.
 //
 // Site records are 4-wide vectors (x, y, z, 0), so a neighbour costs one
 // vector load; neighbours are local slot numbers packed two per 32-bit word;
@@ -31,6 +35,7 @@ struct ClusterParams {
     int pmax;              // push entries per own site
     int ZT;                // edge slots (padded to the kernel's template value)
     int energy_from_field; // must be 1 (host routes other lattices elsewhere)
+    int async_halo;        // halo pushes complete transactions on the receiver's mbarriers
     double h;
     float hf;
     double coef64[kMaxEdgeSlots][3];

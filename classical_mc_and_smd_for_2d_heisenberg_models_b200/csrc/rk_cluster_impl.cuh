@@ -12,8 +12,14 @@
 //   fix:     FP64 field sweep, cluster reduction of sigma and E, S = norm(S +
 //            scale S x (h x S)) for every site from one set of fields, write A
 //
-// "sync" is one cluster barrier (release/acquire), which also orders the
-// distributed-shared-memory pushes.  The FP64 form (T = double) corrects
+// "sync" publishes the halo pushes: with async halo pushes (st.async
+// stores that complete bytes on one of two mbarriers of the receiving CTA,
+// alternating per publish), the next stage waits for its own CTA's halo
+// bytes only; otherwise it is one cluster barrier (release/acquire).  Two
+// barriers suffice: a CTA pushes publish p only after it received publish
+// p-1 from every CTA it pushes to, and the neighbour relation is symmetric,
+// so every reader of a halo copy has read it (and completed its phase p-2)
+// before the copy's owner overwrites it.  The FP64 form (T = double) corrects
 // every step against the energy at the step's start, as the reference does;
 // the FP32 form (T = float) reuses the two FP32 buffers as one FP64 buffer
 // for its correction sweep every fix_every steps, against the initial
@@ -83,6 +89,7 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
     off = (off + 15) & ~size_t(15);
     double *red = reinterpret_cast<double *>(smem_raw + off);   // [2][16][4]
     double *wpart = red + 2 * kMaxClusterCTAs * 4;                // [32][4]
+    uint64_t *hbar = reinterpret_cast<uint64_t *>(wpart + 32 * 4);  // [2] halo publish barriers
     double *D = reinterpret_cast<double *>(smem_raw);             // [3][Np], FP32 form only
 
     // ---- tables
@@ -147,6 +154,56 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
     auto arrive = [&]() { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); };
     auto wait = [&]() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); };
 
+    // Async halo publishes: publish p uses barrier hbar[p & 1] (phase p / 2).
+    // Thread 0 arms it with the CTA's incoming halo bytes when the CTA starts
+    // producing publish p (bytes that arrive first drive the transaction
+    // count negative, which the phase tolerates: it also needs the arrival);
+    // the consumer waits with a bounded poll, flagging the status on expiry.
+    const bool AH = P.async_halo != 0;
+    const uint32_t hbar_a = (uint32_t)__cvta_generic_to_shared(hbar);
+    constexpr uint32_t kHaloBytes = sizeof(T) == 4 ? 16 : 24;   // x, y, z (+ w in FP32)
+    int pub = 0, need = -1;      // next publish; publish the next halo reads need
+    uint32_t cur_bar = hbar_a;
+    auto begin_pub = [&]() {
+        if (!AH) return;
+        cur_bar = hbar_a + (uint32_t)(pub & 1) * 8u;
+        if (tid == 0)
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(cur_bar),
+                         "r"((uint32_t)n_halo * kHaloBytes)
+                         : "memory");
+    };
+    auto end_pub = [&]() {
+        if (AH) {
+            need = pub++;
+        } else {
+            arrive();
+        }
+        __syncthreads();
+    };
+    bool hfail = false;          // a wait expired: later waits return at once
+    auto hwait = [&](int q) {
+        if (q < 0 || hfail) return;
+        const uint32_t a = hbar_a + (uint32_t)(q & 1) * 8u, par = (uint32_t)(q >> 1) & 1u;
+        for (unsigned it = 0; it < (1u << 26); it++) {
+            uint32_t ok;
+            asm volatile(
+                "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
+                " selp.u32 %0, 1, 0, p;\n}\n"
+                : "=r"(ok)
+                : "r"(a), "r"(par)
+                : "memory");
+            if (ok) return;
+        }
+        hfail = true;
+        atomicOr(J.status, 1 << kStatusHaloTimeout);
+    };
+    // the barrier half of a stage: the halo bytes of the publish this stage
+    // reads, or the cluster barrier's wait
+    auto sync_in = [&]() {
+        if (AH) hwait(need);
+        else wait();
+    };
+
     // Sum of NV doubles over every thread of every CTA of the cluster; all
     // threads receive the totals, summed in a fixed order.
     auto cluster_sum = [&](double *v, int NV) {
@@ -178,15 +235,38 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
 
     // local store of own site k's value plus the pushes into halo copies
     // (push codes fill from slot 0, so pc0 < 0 means no pushes at all)
+    auto push1 = [&](Vec4<T> *buf, int code, const Vec4<T> &v) {
+        if (AH) {
+            const uint32_t la = (uint32_t)__cvta_generic_to_shared(buf + (code & 0xffff));
+            uint32_t ra, rb;
+            asm("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(ra) : "r"(la), "r"(code >> 16));
+            asm("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(rb) : "r"(cur_bar), "r"(code >> 16));
+            if constexpr (sizeof(T) == 4) {
+                asm volatile(
+                    "st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.f32 [%0], {%1, %2, %3, %4}, [%5];" ::"r"(ra),
+                    "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w), "r"(rb)
+                    : "memory");
+            } else {
+                asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f64 [%0], {%1, %2}, [%3];" ::"r"(ra),
+                             "d"(v.x), "d"(v.y), "r"(rb)
+                             : "memory");
+                asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.f64 [%0], %1, [%2];" ::"r"(ra + 16u),
+                             "d"(v.z), "r"(rb)
+                             : "memory");
+            }
+        } else {
+            cl.map_shared_rank(buf, code >> 16)[code & 0xffff] = v;
+        }
+    };
     auto put = [&](Vec4<T> *buf, int k, int li, const Vec4<T> &v) {
         buf[li] = v;
         if (pc0[k] >= 0) {
-            cl.map_shared_rank(buf, pc0[k] >> 16)[pc0[k] & 0xffff] = v;
+            push1(buf, pc0[k], v);
             if (pc1[k] >= 0) {
-                cl.map_shared_rank(buf, pc1[k] >> 16)[pc1[k] & 0xffff] = v;
+                push1(buf, pc1[k], v);
                 for (int p = 2; p < P.pmax; p++) {
                     const int code = push[p * nom + li];
-                    if (code >= 0) cl.map_shared_rank(buf, code >> 16)[code & 0xffff] = v;
+                    if (code >= 0) push1(buf, code, v);
                 }
             }
         }
@@ -364,7 +444,12 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
         if (rank == 0 && tid == 0) J.qss[(size_t)smp * J.n_rec + r] = (r == 0) ? 1.0 : (1.0 / N) * v[0];
     };
 
-    cl_sync();   // every CTA of the cluster is running before any remote access
+    if (AH && tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(hbar_a));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(hbar_a + 8u));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    cl_sync();   // every CTA of the cluster is running (barriers initialised) before any remote access
 #pragma unroll
     for (int k = 0; k < SPT; k++) {
         const int li = tid + k * NT;
@@ -391,7 +476,7 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
 #pragma unroll
         for (int k = 0; k < SPT; k++)
             if (own_[k] && !bnd[k]) body(k);
-        wait();
+        sync_in();
 #pragma unroll
         for (int k = 0; k < SPT; k++)
             if (own_[k] && bnd[k]) body(k);
@@ -413,7 +498,7 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
         if (rank == 0 && tid == 0) drift = J.stats[smp * 4 + 0];
     }
     fill(A);
-    arrive();
+    if (!AH) arrive();
     __syncthreads();
 
     const T dt = T(J.dt);
@@ -427,6 +512,7 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
             const bool fix = per_step || (n % F == 0);
             double eref = 0.0;
             // ---- stage 1: A -> B
+            begin_pub();
             two_pass([&](int k) {
                 const int li = tid + k * NT;
                 T h[3], Sp[3], Pv[3];
@@ -448,14 +534,14 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
                 const T m = mk[k];
                 put(B, k, li, {m * Pin[k][0], m * Pin[k][1], m * Pin[k][2], zero});
             });
-            arrive();
-            __syncthreads();
+            end_pub();
             // ---- stages 2 and 3
 #pragma unroll
             for (int stg = 0; stg < 2; stg++) {
                 const Vec4<T> *src = stg ? A : B;
                 Vec4<T> *dst = stg ? B : A;
                 const T cst = stg ? T(1) : T(0.5);
+                begin_pub();
                 two_pass([&](int k) {
                     const int li = tid + k * NT;
                     T h[3], Pv[3];
@@ -476,8 +562,7 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
                     const T m = mk[k];
                     put(dst, k, li, {m * nx[0], m * nx[1], m * nx[2], zero});
                 });
-                arrive();
-                __syncthreads();
+                end_pub();
             }
             // ---- stage 4 and the FP64 combination (reads B, writes nothing
             // shared, so no barrier follows)
@@ -500,19 +585,25 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
                 sync_spin(k);
             });
             if (!fix) {
+                begin_pub();
                 publishA();
-                arrive();
-                __syncthreads();
+                end_pub();
                 continue;
             }
             // ---- energy correction
             if (sizeof(T) == 4) {
                 cl_sync();      // stage-4 reads of B finish before D (over A and B) is written
                 publishD();
+                cl_sync();
+            } else if (AH) {
+                begin_pub();
+                publishA();
+                end_pub();
+                hwait(need);
             } else {
                 publishA();
+                cl_sync();
             }
-            cl_sync();
             double sig = 0.0, e1 = 0.0;
 #pragma unroll
             for (int k = 0; k < SPT; k++) {
@@ -563,16 +654,23 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
                     sync_spin(k);
                 }
             }
+            begin_pub();
             publishA();   // the reduction's cluster barrier ordered every read of A / D before this
+            end_pub();
+        }
+        if (AH) {
+            record(r);
+        } else {
+            wait();   // completes the step's barrier before record's own reduction
+            record(r);
             arrive();
             __syncthreads();
         }
-        wait();   // completes the step's barrier before record's own reduction
-        record(r);
-        arrive();
-        __syncthreads();
     }
-    wait();
+    // the last publish has arrived (async pushes: none is left in flight
+    // towards this CTA when it reaches the final cluster barrier)
+    if (AH) hwait(need);
+    else wait();
 
     double *stw = J.state + (size_t)smp * 3 * N;
 #pragma unroll

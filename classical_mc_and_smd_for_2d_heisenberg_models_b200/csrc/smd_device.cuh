@@ -61,7 +61,10 @@ struct RKJob {
     int bf_kp;
 };
 
-enum { kStatusOK = 0, kStatusBadSigma = 1 };
+// status bits (1 << k): zero correction denominator; bounded waits that
+// expired in the tensor-core projection (2), the time transform (3) and
+// the cluster RK kernel's halo exchange (4)
+enum { kStatusOK = 0, kStatusBadSigma = 1, kStatusHaloTimeout = 4 };
 
 // Mixed-radix factorisation of a transform length (product of radix = n).
 struct FFTPlan {

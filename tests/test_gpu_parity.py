@@ -377,6 +377,31 @@ def test_cluster_vacancies_match_oracle(ctx, oracle_mod, cluster_size):
     assert np.max(np.abs(r.spec - acc)) <= SPEC_TOL * np.max(np.abs(acc))
 
 
+@pytest.mark.parametrize("geom,L,cs", [("triang", 48, 2), ("triang", 48, 16), ("hexagn", 24, 4),
+                                        ("square", 32, 8)])
+@pytest.mark.parametrize("precision", [_lib.SMD_FP64, _lib.SMD_FP32])
+def test_async_halo_equals_cluster_barrier_halo(ctx, cluster_size, monkeypatch, geom, L, cs, precision):
+    """Halo publishes through st.async stores completing on the receiver's
+    mbarriers (the default) and through cluster barriers (SMD_RK_HALO=barrier)
+    move the same values: identical trajectories and spectra over several
+    record chunks, energy corrections included."""
+    cluster_size(cs)
+    s = SMDSettings(geom=geom, L=L, J2=0.12, JX=0.05, h=0.1, imp_ratio=0.05 if geom == "square" else 0.0,
+                    dtm=0.02, ntm=150, NMeas=2000)
+    lat, lid = _upload(ctx, s)
+    qid = ctx.qset(lid)
+    kind = {"triang": "q120", "square": "stripe"}.get(geom, "ferro")
+    spins, imp = smp.make_samples(s, 3, kind, 0.15, 11)
+    impr = None if imp is None else np.tile(imp[0], (3, 1))
+    kw = dict(stride=4, precision=precision, fix_every=16 if precision == _lib.SMD_FP32 else 1, imp=impr)
+    a = ctx.run(lid, qid, spins, s.dtm, 150, **kw)
+    monkeypatch.setenv("SMD_RK_HALO", "barrier")
+    b = ctx.run(lid, qid, spins, s.dtm, 150, **kw)
+    assert a.report["rk_kind"] == 1 and a.report["rk_ctas"] == cs
+    assert np.array_equal(a.final, b.final)
+    assert np.array_equal(a.spec, b.spec) and np.array_equal(a.qss, b.qss)
+
+
 def test_invalid_jobs_fail_loudly(ctx):
     s = SMDSettings(geom="square", L=8, J2=0.6, dtm=0.01, ntm=16)
     lat, lid = _upload(ctx, s)
