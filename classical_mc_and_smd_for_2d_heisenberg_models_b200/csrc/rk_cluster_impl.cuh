@@ -44,6 +44,30 @@ struct alignas(4 * sizeof(T)) Vec4 {
     T x, y, z, w;
 };
 
+// FP64 master spins of a thread's own sites, S[k][c].  The FP32 form keeps
+// them in shared memory ([3][n_own_max], site-fastest, so a warp's accesses
+// are coalesced): they are read only at the RK combination, the corrections
+// and the records, and the registers go to the stage values.  The FP64 form
+// keeps them in registers, where every stage reads them.
+struct MasterRow {
+    double *p;
+    int stride;
+    __device__ __forceinline__ double &operator[](int c) const { return p[c * stride]; }
+};
+struct MasterSmem {
+    double *base;
+    int stride, NT;
+    __device__ __forceinline__ MasterRow operator[](int k) const
+    {
+        return {base + threadIdx.x + k * NT, stride};
+    }
+};
+template <int SPT>
+struct MasterRegs {
+    double v[SPT][3];
+    __device__ __forceinline__ double (&operator[](int k))[3] { return v[k]; }
+};
+
 __device__ __forceinline__ double cl_coef(const ClusterParams &P, int e, int c, double)
 {
     return P.coef64[e][c];
@@ -90,6 +114,7 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
     double *red = reinterpret_cast<double *>(smem_raw + off);   // [2][16][4]
     double *wpart = red + 2 * kMaxClusterCTAs * 4;                // [32][4]
     uint64_t *hbar = reinterpret_cast<uint64_t *>(wpart + 32 * 4);  // [2] halo publish barriers
+    double *Sm = reinterpret_cast<double *>(hbar + 2);              // [3][nom], FP32 form only
     double *D = reinterpret_cast<double *>(smem_raw);             // [3][Np], FP32 form only
 
     // ---- tables
@@ -103,7 +128,9 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
     const double *st = J.state + (size_t)smp * 3 * N;
     const uint8_t *imp = J.imp ? J.imp + (size_t)smp * N : nullptr;
 
-    double S[SPT][3];
+    constexpr bool SF = sizeof(T) == 4;
+    std::conditional_t<SF, MasterSmem, MasterRegs<SPT>> S;
+    if constexpr (SF) S = MasterSmem{Sm, nom, NT};
     T mk[SPT];
 #pragma unroll
     for (int k = 0; k < SPT; k++) {
@@ -114,8 +141,9 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
             for (int c = 0; c < 3; c++) S[k][c] = st[c * N + g];
             mk[k] = (imp && imp[g]) ? zero : T(1);
         } else {
+            if constexpr (!SF)
 #pragma unroll
-            for (int c = 0; c < 3; c++) S[k][c] = 0.0;
+                for (int c = 0; c < 3; c++) S[k][c] = 0.0;
             mk[k] = zero;
         }
     }
@@ -123,7 +151,6 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
     const double hz = P.h;
     // FP32 copy of the master spins (FP32 form): stage inputs need no
     // conversion from FP64 at every stage
-    constexpr bool SF = sizeof(T) == 4;
     T Sf[SF ? SPT : 1][3];
     auto spin = [&](int k, int c) -> T {
         if constexpr (SF) return Sf[k][c];
@@ -135,7 +162,11 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
             for (int c = 0; c < 3; c++) Sf[k][c] = T(S[k][c]);
     };
 #pragma unroll
-    for (int k = 0; k < SPT; k++) sync_spin(k);
+    for (int k = 0; k < SPT; k++) {
+        if (tid + k * NT < n_own) sync_spin(k);
+        else if constexpr (SF)
+            for (int c = 0; c < 3; c++) Sf[k][c] = zero;
+    }
     // packed neighbour words and the first two push codes of each own site
     // live in registers (after the table load below); further push codes
     // stay in shared memory
