@@ -308,8 +308,12 @@ extern "C" int smd_ctx_create(const smd_device_opts *opts, smd_ctx **out)
     size_t fr = 0, tot = 0;
     CK(cudaMemGetInfo(&fr, &tot), "cudaMemGetInfo");
     c->budget = (opts && opts->hbm_budget) ? opts->hbm_budget : (size_t)(0.85 * (double)fr);
-    CK(cudaStreamCreateWithFlags(&c->s_rk, cudaStreamNonBlocking), "stream");
-    CK(cudaStreamCreateWithFlags(&c->s_proj, cudaStreamNonBlocking), "stream");
+    // the integration stream is on the critical path: its launches take SMs
+    // ahead of the projection's blocks as they free up
+    int prio_lo = 0, prio_hi = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi), "stream priorities");
+    CK(cudaStreamCreateWithPriority(&c->s_rk, cudaStreamNonBlocking, prio_hi), "stream");
+    CK(cudaStreamCreateWithPriority(&c->s_proj, cudaStreamNonBlocking, prio_lo), "stream");
     for (int i = 0; i < 2; i++) {
         CK(cudaEventCreateWithFlags(&c->ev_rk[i], cudaEventDisableTiming), "event");
         CK(cudaEventCreateWithFlags(&c->ev_proj[i], cudaEventDisableTiming), "event");
