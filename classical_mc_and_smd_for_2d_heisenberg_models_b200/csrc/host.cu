@@ -118,11 +118,17 @@ struct Plan {
 
 }  // namespace
 
+// Snapshot buffers between the integration and projection streams: the RK
+// launch of chunk c reuses the buffer of chunk c - kSnapBufs, so the
+// projection has kSnapBufs - 1 RK launches' time to catch up before the
+// integration waits for it.
+constexpr int kSnapBufs = 3;
+
 struct smd_ctx {
     int device = 0;
     size_t budget = 0;
     cudaStream_t s_rk = nullptr, s_proj = nullptr;
-    cudaEvent_t ev_rk[2] = {nullptr, nullptr}, ev_proj[2] = {nullptr, nullptr};
+    cudaEvent_t ev_rk[kSnapBufs]{}, ev_proj[kSnapBufs]{};
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     std::string err;
     int next_id = 1;
@@ -133,16 +139,16 @@ struct smd_ctx {
     std::map<int, std::shared_ptr<QSet>> qsets;
     std::map<int, std::unique_ptr<Plan>> tplans;   // keyed by n
     // job buffers (grow-only)
-    DevBuf state, s0, imp, snap[2], series, qss, stats, e0, status, win, acc_tmp, in_tmp, out_tmp;
+    DevBuf state, s0, imp, snap[kSnapBufs], series, qss, stats, e0, status, win, acc_tmp, in_tmp, out_tmp;
     DevBuf gscratch;   // packed row-transformed grids of the two-pass grid transform
     int launches = 0;
     std::vector<cudaEvent_t> tev;   // timing events, reused across calls
-    // bf16 high / low parts of one chunk's snapshot rows and their maps
-    // split-BF16 snapshot rows, one pair per snapshot buffer
-    DevBuf ahi[2], alo[2];
-    CUtensorMap map_ahi[2]{}, map_alo[2]{};
-    const void *map_a_base[2] = {nullptr, nullptr};
-    int map_a_rows[2] = {0, 0}, map_a_kp[2] = {0, 0};
+    // split-BF16 snapshot rows and their tensor maps, one pair per snapshot
+    // buffer
+    DevBuf ahi[kSnapBufs], alo[kSnapBufs];
+    CUtensorMap map_ahi[kSnapBufs]{}, map_alo[kSnapBufs]{};
+    const void *map_a_base[kSnapBufs]{};
+    int map_a_rows[kSnapBufs]{}, map_a_kp[kSnapBufs]{};
 };
 
 namespace {
@@ -314,7 +320,7 @@ extern "C" int smd_ctx_create(const smd_device_opts *opts, smd_ctx **out)
     CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi), "stream priorities");
     CK(cudaStreamCreateWithPriority(&c->s_rk, cudaStreamNonBlocking, prio_hi), "stream");
     CK(cudaStreamCreateWithPriority(&c->s_proj, cudaStreamNonBlocking, prio_lo), "stream");
-    for (int i = 0; i < 2; i++) {
+    for (int i = 0; i < kSnapBufs; i++) {
         CK(cudaEventCreateWithFlags(&c->ev_rk[i], cudaEventDisableTiming), "event");
         CK(cudaEventCreateWithFlags(&c->ev_proj[i], cudaEventDisableTiming), "event");
     }
@@ -332,7 +338,7 @@ extern "C" int smd_ctx_destroy(smd_ctx *ctx)
     ctx->lattices.clear();
     ctx->qsets.clear();
     ctx->tplans.clear();
-    for (int i = 0; i < 2; i++) {
+    for (int i = 0; i < kSnapBufs; i++) {
         cudaEventDestroy(ctx->ev_rk[i]);
         cudaEventDestroy(ctx->ev_proj[i]);
     }
@@ -907,7 +913,10 @@ int prepare(smd_ctx *ctx, const smd_job_desc *job, JobGeom &g)
     // per-sample device bytes
     const size_t N = g.N;
     const bool large = g.Qs->use_grid && g.Qs->large[g.prec == SMD_FP64 ? 0 : 1];
-    const size_t per = 2 * 3 * N * sizeof(double) + N + 2 * (size_t)g.R * 3 * N * g.elem +
+    // FP32 list projection on tensor cores: split-BF16 rows beside every
+    // snapshot buffer
+    const size_t bf_rows = (g.Qs->n_list > 0 && g.prec == SMD_FP32) ? (size_t)g.R * 3 * g.Qs->kp * 4 : 0;
+    const size_t per = 2 * 3 * N * sizeof(double) + N + kSnapBufs * ((size_t)g.R * 3 * N * g.elem + bf_rows) +
                        3 * (size_t)g.n_rec * g.nqb * 16 + (size_t)g.n_rec * sizeof(double) +
                        5 * sizeof(double) +
                        (large ? grid_large_scratch(g.Qs->G, g.R, g.prec == SMD_FP64 ? 0 : 1) : 0);
@@ -932,7 +941,7 @@ int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const do
     CK(ctx->state.ensure((size_t)W * 3 * N * sizeof(double)), "cudaMalloc state");
     CK(ctx->s0.ensure((size_t)W * 3 * N * sizeof(double)), "cudaMalloc s0");
     CK(ctx->imp.ensure((size_t)W * N), "cudaMalloc imp");
-    for (int b = 0; b < 2; b++)
+    for (int b = 0; b < kSnapBufs; b++)
         CK(ctx->snap[b].ensure((size_t)W * R * 3 * N * g.elem), "cudaMalloc snap");
     CK(ctx->series.ensure((size_t)W * 3 * n_rec * nqb * 16), "cudaMalloc series");
     CK(ctx->qss.ensure((size_t)W * n_rec * sizeof(double)), "cudaMalloc qss");
@@ -979,9 +988,9 @@ int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const do
         // the proj stream must not overwrite series of the previous wave
         // before its time transform finished: both run on s_proj in order.
         for (int c = 0; c < nchunks; c++) {
-            const int b = c & 1;
+            const int b = c % kSnapBufs;
             const int rb = c * R, re = std::min(n_rec, rb + R);
-            if (c >= 2) CK(cudaStreamWaitEvent(ctx->s_rk, ctx->ev_proj[b], 0), "wait");
+            if (c >= kSnapBufs) CK(cudaStreamWaitEvent(ctx->s_rk, ctx->ev_proj[b], 0), "wait");
             RKJob J{};
             J.n_samples = Ww;
             J.dt = job->dt;
@@ -1090,7 +1099,7 @@ int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const do
                            ctx->status.as<int>(), ctx->s_proj), "time fft");
         CK(cudaEventRecord(ev(nev - 1), ctx->s_proj), "event");
         ctx->launches++;
-        CK(cudaStreamWaitEvent(ctx->s_proj, ctx->ev_rk[(nchunks - 1) & 1], 0), "wait");
+        CK(cudaStreamWaitEvent(ctx->s_proj, ctx->ev_rk[(nchunks - 1) % kSnapBufs], 0), "wait");
         CK(launch_sum_rows(ctx->qss.as<double>(), Ww, n_rec, d_qss_sum, ctx->s_proj), "qss");
         ctx->launches++;
         if (d_final) {
