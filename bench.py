@@ -35,17 +35,29 @@ METRIC = "SMD site-steps/s"
 UNIT = "site-steps/s"
 
 
-def profile_traffic(name: str):
+def profile_traffic(name: str, records_per_launch: float = 0.0):
     """DRAM bytes (read + write) per launch of a kernel from its committed
-    ncu summary in profiles/ (the `dram_bytes_per_launch:` line), or None."""
+    ncu summary in profiles/ (the `dram_bytes_per_launch:` line), or None.
+    A summary with a `records_per_launch:` line was captured on launches of
+    that many records; its bytes scale to `records_per_launch` (the traffic
+    is the per-record snapshot and operand-row writes)."""
     path = os.path.join(ROOT, "profiles", name)
+    traffic, rec = None, 0
     try:
         for line in open(path):
             if line.startswith("dram_bytes_per_launch:"):
-                return int(line.split(":")[1]), f"profiles/{name}"
+                traffic = int(line.split(":")[1])
+            elif line.startswith("records_per_launch:"):
+                rec = int(line.split(":")[1])
     except OSError:
-        pass
-    return None, None
+        return None, None
+    if traffic is None:
+        return None, None
+    src = f"profiles/{name}"
+    if rec and records_per_launch and records_per_launch != rec:
+        traffic = int(round(traffic * records_per_launch / rec))
+        src += f" (captured at {rec} records per launch, scaled to {records_per_launch:g})"
+    return traffic, src
 
 
 def flops_per_site_step(z: int) -> int:
@@ -350,7 +362,9 @@ def run_ours(args, w, rank, world):
     prec_peak = lib.smd_measure_fma_peak(local, w.precision, C.byref(peak))
     rk_flops = fpss * site_steps_rank * args.steps
     achieved = rk_flops / (ms_rk / 1e3) / 1e12
-    traffic, traffic_src = profile_traffic(f"{rk_kind}_{w.name}.md")
+    waves = max(1, reps[-1].waves)
+    traffic, traffic_src = profile_traffic(f"{rk_kind}_{w.name}.md",
+                                           w.n_rec * waves * args.steps / max(1, rk_launches))
     roof = {"kernel": rk_kind,
             "bound": "fp32" if w.precision == _lib.SMD_FP32 else "fp64",
             "achieved": achieved, "peak": peak.value if prec_peak == 0 else None,
