@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(MAXT, MINB) grid_proj_kernel(
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int QB = series_qb<T>();
-    const int G = plan.n, GG = G * G, NGG = NG * GG, P = G + 1;
+    const int G = plan.n, GG = G * G, P = G + 1;
     cplx<T> *buf = reinterpret_cast<cplx<T> *>(smem_raw);
     cplx<T> *tw = buf + NG * G * P;
     cplx<T> *scratch = (FL & FK_GEN) ? tw + G : nullptr;
@@ -56,17 +56,24 @@ __global__ void __launch_bounds__(MAXT, MINB) grid_proj_kernel(
     const TS *x0 = snap + ((size_t)(s * R + slot0) * 3 + g0) * N;
     const TS *x1 = x0 + 3 * (size_t)N;   // the next slot
     for (int k = threadIdx.x; k < G; k += blockDim.x) tw[k] = tw_g[k];
-#pragma unroll 4
-    for (int p = threadIdx.x; p < NGG; p += blockDim.x) {
-        const int g = p / GG, rem = p - g * GG;
+    // one grid-map load serves the NG components of both records
+#pragma unroll 2
+    for (int rem = threadIdx.x; rem < GG; rem += blockDim.x) {
         const int idx = grid_map[rem];
-        T a = T(0), b = T(0);
-        if (idx >= 0) {
-            a = T(x0[(size_t)g * N + idx]);
-            if (has1) b = T(x1[(size_t)g * N + idx]);
-        }
         const int r = rem / G, col = rem - r * G;
-        buf[(r * NG + g) * P + col] = {a, b};
+        T a[3], b[3];
+#pragma unroll
+        for (int g = 0; g < 3; g++) {
+            a[g] = T(0);
+            b[g] = T(0);
+            if (g < NG && idx >= 0) {
+                a[g] = T(x0[(size_t)g * N + idx]);
+                if (has1) b[g] = T(x1[(size_t)g * N + idx]);
+            }
+        }
+#pragma unroll
+        for (int g = 0; g < 3; g++)
+            if (g < NG) buf[(r * NG + g) * P + col] = {a[g], b[g]};
     }
     __syncthreads();
     if constexpr (P1 > 0) {
