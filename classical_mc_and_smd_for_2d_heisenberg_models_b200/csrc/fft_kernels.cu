@@ -579,7 +579,7 @@ bool time_fft_fits(int n, int precision, const FFTPlan &p)
 
 cudaError_t launch_time_fft(const void *series, int precision, int W, int Q, int nqb,
                             const FFTPlan &plan, const void *tw, double *acc, int *status,
-                            cudaStream_t st)
+                            cudaStream_t st, int ncomp)
 {
     const int n = plan.n;
     const int qb = series_qblock(precision);
@@ -592,12 +592,12 @@ cudaError_t launch_time_fft(const void *series, int precision, int W, int Q, int
         if (precision == 0) {
             auto k = time_fft_pow2_kernel<double>;
             allow_dynamic_smem(k);
-            k<<<3 * ntile, threads, smem, st>>>((const cplx<double> *)series, W, Q, nqb, n, l2, nseq,
+            k<<<ncomp * ntile, threads, smem, st>>>((const cplx<double> *)series, W, Q, nqb, n, l2, nseq,
                                                 (const cplx<double> *)tw, acc, status);
         } else {
             auto k = time_fft_pow2_kernel<float>;
             allow_dynamic_smem(k);
-            k<<<3 * ntile, threads, smem, st>>>((const cplx<float> *)series, W, Q, nqb, n, l2, nseq,
+            k<<<ncomp * ntile, threads, smem, st>>>((const cplx<float> *)series, W, Q, nqb, n, l2, nseq,
                                                 (const cplx<float> *)tw, acc, status);
         }
         return cudaGetLastError();
@@ -610,12 +610,12 @@ cudaError_t launch_time_fft(const void *series, int precision, int W, int Q, int
     if (precision == 0) {
         auto k = time_kernel<double>(fl);
         allow_dynamic_smem(k);
-        k<<<3 * ntile, threads, smem, st>>>((const cplx<double> *)series, W, Q, nqb, qt, plan,
+        k<<<ncomp * ntile, threads, smem, st>>>((const cplx<double> *)series, W, Q, nqb, qt, plan,
                                             (const cplx<double> *)tw, acc, gen);
     } else {
         auto k = time_kernel<float>(fl);
         allow_dynamic_smem(k);
-        k<<<3 * ntile, threads, smem, st>>>((const cplx<float> *)series, W, Q, nqb, qt, plan,
+        k<<<ncomp * ntile, threads, smem, st>>>((const cplx<float> *)series, W, Q, nqb, qt, plan,
                                             (const cplx<float> *)tw, acc, gen);
     }
     return cudaGetLastError();

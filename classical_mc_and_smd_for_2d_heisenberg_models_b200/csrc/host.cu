@@ -129,6 +129,7 @@ struct smd_ctx {
     size_t budget = 0;
     cudaStream_t s_rk = nullptr, s_proj = nullptr;
     cudaEvent_t ev_rk[kSnapBufs]{}, ev_proj[kSnapBufs]{};
+    cudaEvent_t ev_tf[3]{};   // per-component time transforms done (host copy may start)
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     std::string err;
     int next_id = 1;
@@ -320,6 +321,7 @@ extern "C" int smd_ctx_create(const smd_device_opts *opts, smd_ctx **out)
     CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi), "stream priorities");
     CK(cudaStreamCreateWithPriority(&c->s_rk, cudaStreamNonBlocking, prio_hi), "stream");
     CK(cudaStreamCreateWithPriority(&c->s_proj, cudaStreamNonBlocking, prio_lo), "stream");
+    for (int i = 0; i < 3; i++) CK(cudaEventCreateWithFlags(&c->ev_tf[i], cudaEventDisableTiming), "event");
     for (int i = 0; i < kSnapBufs; i++) {
         CK(cudaEventCreateWithFlags(&c->ev_rk[i], cudaEventDisableTiming), "event");
         CK(cudaEventCreateWithFlags(&c->ev_proj[i], cudaEventDisableTiming), "event");
@@ -338,6 +340,7 @@ extern "C" int smd_ctx_destroy(smd_ctx *ctx)
     ctx->lattices.clear();
     ctx->qsets.clear();
     ctx->tplans.clear();
+    for (int i = 0; i < 3; i++) cudaEventDestroy(ctx->ev_tf[i]);
     for (int i = 0; i < kSnapBufs; i++) {
         cudaEventDestroy(ctx->ev_rk[i]);
         cudaEventDestroy(ctx->ev_proj[i]);
@@ -934,7 +937,7 @@ int prepare(smd_ctx *ctx, const smd_job_desc *job, JobGeom &g)
 // The pipeline of one job on device buffers; spec/qss sums accumulate.
 int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const double *d_spins0,
                const double *d_win, double *d_spec_sum, double *d_qss_sum, double *d_final,
-               smd_report *rep)
+               smd_report *rep, double *h_spec = nullptr, double fc = 1.0)
 {
     const int N = g.N, Q = g.Q, nqb = g.nqb, n_rec = g.n_rec, R = g.R, W = g.W;
     Lattice &L = *g.L;
@@ -1095,11 +1098,35 @@ int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const do
             CK(cudaEventRecord(ctx->ev_proj[b], ctx->s_proj), "event");
         }
         CK(cudaEventRecord(ev(nev - 2), ctx->s_proj), "event");
-        CK(launch_time_fft(ctx->series.p, g.prec, Ww, Q, nqb, g.tp->p,
-                           g.prec == SMD_FP64 ? g.tp->tw64.p : g.tp->tw32.p, d_spec_sum,
-                           ctx->status.as<int>(), ctx->s_proj), "time fft");
-        CK(cudaEventRecord(ev(nev - 1), ctx->s_proj), "event");
-        ctx->launches++;
+        const void *tw = g.prec == SMD_FP64 ? g.tp->tw64.p : g.tp->tw32.p;
+        if (h_spec && w == g.waves - 1) {
+            // last wave with a host destination: one transform per spin
+            // component, each scaled by fc and copied to the host on the RK
+            // stream (idle by now) while the next component transforms
+            const size_t comp_series = (size_t)nqb * n_rec * 16, comp_acc = (size_t)Q * n_rec;
+            for (int c = 0; c < 3; c++) {
+                CK(launch_time_fft(static_cast<const char *>(ctx->series.p) + c * comp_series, g.prec, Ww, Q,
+                                   nqb, g.tp->p, tw, d_spec_sum + c * comp_acc, ctx->status.as<int>(),
+                                   ctx->s_proj, 1),
+                   "time fft");
+                CK(launch_scale(d_spec_sum + c * comp_acc, comp_acc, fc, ctx->s_proj), "scale");
+                CK(cudaEventRecord(ctx->ev_tf[c], ctx->s_proj), "event");
+                ctx->launches += 2;
+            }
+            CK(cudaEventRecord(ev(nev - 1), ctx->s_proj), "event");
+            for (int c = 0; c < 3; c++) {
+                CK(cudaStreamWaitEvent(ctx->s_rk, ctx->ev_tf[c], 0), "wait");
+                CK(cudaMemcpyAsync(h_spec + c * comp_acc, d_spec_sum + c * comp_acc, comp_acc * sizeof(double),
+                                   cudaMemcpyDeviceToHost, ctx->s_rk),
+                   "D2H spec");
+            }
+        } else {
+            CK(launch_time_fft(ctx->series.p, g.prec, Ww, Q, nqb, g.tp->p, tw, d_spec_sum,
+                               ctx->status.as<int>(), ctx->s_proj),
+               "time fft");
+            CK(cudaEventRecord(ev(nev - 1), ctx->s_proj), "event");
+            ctx->launches++;
+        }
         CK(cudaStreamWaitEvent(ctx->s_proj, ctx->ev_rk[(nchunks - 1) % kSnapBufs], 0), "wait");
         CK(launch_sum_rows(ctx->qss.as<double>(), Ww, n_rec, d_qss_sum, ctx->s_proj), "qss");
         ctx->launches++;
@@ -1198,15 +1225,15 @@ extern "C" int smd_run(smd_ctx *ctx, const smd_job_desc *job, const double *spin
     CK(cudaMemsetAsync(d_acc, 0, acc_b + n * sizeof(double), ctx->s_rk), "memset");
     CK(cudaStreamSynchronize(ctx->s_rk), "sync");
     auto w1 = std::chrono::steady_clock::now();
+    // averages over samples on the device, as the reference's fc = 1 / evoCnt
+    // (smd_code.cpp:3596-3611); the last wave scales each component's
+    // spectrum and copies it to spec_out while the next one transforms
+    const double fc = 1.0 / (double)S;
     rc = run_device(ctx, job, g, d_in, d_win, d_acc, d_q, out_b ? ctx->out_tmp.as<double>() : nullptr,
-                    rep);
+                    rep, spec_out, fc);
     if (rc) return rc;
     auto w2 = std::chrono::steady_clock::now();
-    // average over samples on the device, as the reference's fc = 1 / evoCnt
-    // (smd_code.cpp:3596-3611), then one copy of each output
-    const double fc = 1.0 / (double)S;
-    CK(launch_scale(d_acc, 3 * Q * n + n, fc, ctx->s_rk), "scale");
-    CK(cudaMemcpyAsync(spec_out, d_acc, acc_b, cudaMemcpyDeviceToHost, ctx->s_rk), "D2H spec");
+    CK(launch_scale(d_q, n, fc, ctx->s_rk), "scale");
     CK(cudaMemcpyAsync(qss_out, d_q, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->s_rk), "D2H qss");
     if (out_b)
         CK(cudaMemcpyAsync(final_out, ctx->out_tmp.p, out_b, cudaMemcpyDeviceToHost, ctx->s_rk), "D2H final");

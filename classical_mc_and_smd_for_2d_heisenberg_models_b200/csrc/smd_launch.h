@@ -38,9 +38,11 @@ int time_fft_qt(int n, int precision);
 size_t time_fft_smem(int n, int qt, int precision, const FFTPlan &p);
 // whether the shared-memory time transform takes length n
 bool time_fft_fits(int n, int precision, const FFTPlan &p);
+// ncomp: spin components transformed (3; 1 with series and acc offset to
+// one component's rows)
 cudaError_t launch_time_fft(const void *series, int precision, int W, int Q, int nqb,
                             const FFTPlan &plan, const void *tw, double *acc, int *status,
-                            cudaStream_t st);
+                            cudaStream_t st, int ncomp = 3);
 cudaError_t launch_aos_to_soa(const double *in, double *out, int W, int N, cudaStream_t st);
 cudaError_t launch_soa_to_aos(const double *in, double *out, int W, int N, cudaStream_t st);
 cudaError_t launch_sum_rows(const double *rows, int W, int n, double *out, cudaStream_t st);
