@@ -142,6 +142,7 @@ struct smd_ctx {
     // job buffers (grow-only)
     DevBuf state, s0, imp, snap[kSnapBufs], series, qss, stats, e0, status, win, acc_tmp, in_tmp, out_tmp;
     DevBuf gscratch;   // packed row-transformed grids of the two-pass grid transform
+    DevBuf qpart;      // cluster kernel: per-CTA autocorrelation partials [W][n_rec][CS]
     int launches = 0;
     std::vector<cudaEvent_t> tev;   // timing events, reused across calls
     // split-BF16 snapshot rows and their tensor maps, one pair per snapshot
@@ -922,7 +923,7 @@ int prepare(smd_ctx *ctx, const smd_job_desc *job, JobGeom &g)
     const size_t bf_rows = (g.Qs->n_list > 0 && g.prec == SMD_FP32) ? (size_t)g.R * 3 * g.Qs->kp * 4 : 0;
     const size_t per = 2 * 3 * N * sizeof(double) + N + kSnapBufs * ((size_t)g.R * 3 * N * g.elem + bf_rows) +
                        3 * (size_t)g.n_rec * g.nqb * 16 + (size_t)g.n_rec * sizeof(double) +
-                       5 * sizeof(double) +
+                       5 * sizeof(double) + (size_t)g.n_rec * kMaxClusterCTAs * sizeof(double) +
                        (large ? grid_large_scratch(g.Qs->G, g.R, g.prec == SMD_FP64 ? 0 : 1) : 0);
     const size_t fixed = 3 * (size_t)g.Q * g.n_rec * sizeof(double) + (64u << 20);
     if (ctx->budget <= fixed + per) return fail(ctx, SMD_ENOMEM_ADMIT, "job: one sample exceeds the HBM budget");
@@ -949,6 +950,8 @@ int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const do
         CK(ctx->snap[b].ensure((size_t)W * R * 3 * N * g.elem), "cudaMalloc snap");
     CK(ctx->series.ensure((size_t)W * 3 * n_rec * nqb * 16), "cudaMalloc series");
     CK(ctx->qss.ensure((size_t)W * n_rec * sizeof(double)), "cudaMalloc qss");
+    if (g.ctab && !g.rows)
+        CK(ctx->qpart.ensure((size_t)W * n_rec * g.ctab->P.CS * sizeof(double)), "cudaMalloc qpart");
     CK(ctx->stats.ensure((size_t)W * 4 * sizeof(double)), "cudaMalloc stats");
     CK(ctx->e0.ensure((size_t)W * sizeof(double)), "cudaMalloc e0");
     CK(ctx->status.ensure(sizeof(int)), "cudaMalloc status");
@@ -1012,6 +1015,7 @@ int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const do
             J.qss = ctx->qss.as<double>();
             J.stats = ctx->stats.as<double>();
             J.status = ctx->status.as<int>();
+            J.qpart = (g.ctab && !g.rows) ? ctx->qpart.as<double>() : nullptr;
             // the cluster kernel writes the tensor-core operand rows itself
             const bool tc_list = Qs.n_list > 0 && g.prec == SMD_FP32;
             const bool fused_split = tc_list && g.ctab && !g.rows;
@@ -1128,6 +1132,12 @@ int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const do
             ctx->launches++;
         }
         CK(cudaStreamWaitEvent(ctx->s_proj, ctx->ev_rk[(nchunks - 1) % kSnapBufs], 0), "wait");
+        if (g.ctab && !g.rows) {
+            CK(launch_qss_from_parts(ctx->qpart.as<double>(), Ww, n_rec, g.ctab->P.CS, N, ctx->qss.as<double>(),
+                                     ctx->s_proj),
+               "qss");
+            ctx->launches++;
+        }
         CK(launch_sum_rows(ctx->qss.as<double>(), Ww, n_rec, d_qss_sum, ctx->s_proj), "qss");
         ctx->launches++;
         if (d_final) {

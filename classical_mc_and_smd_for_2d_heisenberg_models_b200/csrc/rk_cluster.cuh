@@ -49,6 +49,10 @@ struct ClusterParams {
 };
 
 size_t rk_cluster_smem(const ClusterParams &P, int precision);
+// qss[s][r] = r == 0 ? 1 : (1 / N) * sum over the CS partials of record r,
+// summed in rank order (the order of the in-cluster reduction)
+cudaError_t launch_qss_from_parts(const double *qpart, int W, int n_rec, int CS, int N, double *qss,
+                                  cudaStream_t st);
 int rk_cluster_maxt(int precision, int spt);
 cudaError_t launch_rk_cluster(const ClusterParams &P, const RKJob &J, int precision, int spt,
                               int threads, cudaStream_t st);

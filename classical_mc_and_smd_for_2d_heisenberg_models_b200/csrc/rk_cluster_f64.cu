@@ -18,6 +18,24 @@ size_t rk_cluster_smem(const ClusterParams &P, int precision)
     return b + (precision == 0 ? 0 : (size_t)3 * P.n_own_max * sizeof(double));
 }
 
+__global__ void qss_from_parts_kernel(const double *__restrict__ qpart, int W, int n_rec, int CS, int N,
+                                      double *__restrict__ qss)
+{
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (size_t)W * n_rec) return;
+    double s = 0.0;
+    for (int r = 0; r < CS; r++) s += qpart[e * CS + r];
+    qss[e] = (e % n_rec == 0) ? 1.0 : (1.0 / N) * s;
+}
+
+cudaError_t launch_qss_from_parts(const double *qpart, int W, int n_rec, int CS, int N, double *qss,
+                                  cudaStream_t st)
+{
+    const size_t n = (size_t)W * n_rec;
+    qss_from_parts_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(qpart, W, n_rec, CS, N, qss);
+    return cudaGetLastError();
+}
+
 int rk_cluster_maxt(int precision, int spt)
 {
     return precision == 0 ? cl_maxt<double>(spt) : cl_maxt<float>(spt);

@@ -470,6 +470,20 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
                 }
             }
         }
+        if (J.qpart) {
+            // this CTA's partial, summed over the cluster by a later launch:
+            // no cluster barrier at a record
+            const int lane = tid & 31, warp = tid >> 5, nw = (NT + 31) >> 5;
+            const double x = warp_sum(p);
+            if (lane == 0) wpart[warp * 4] = x;
+            __syncthreads();
+            if (warp == 0) {
+                const double y = warp_sum((lane < nw) ? wpart[lane * 4] : 0.0);
+                if (lane == 0) J.qpart[((size_t)smp * J.n_rec + r) * CS + rank] = y;
+            }
+            __syncthreads();   // wpart is read before the next reduction writes it
+            return;
+        }
         double v[1] = {p};
         cluster_sum(v, 1);
         if (rank == 0 && tid == 0) J.qss[(size_t)smp * J.n_rec + r] = (r == 0) ? 1.0 : (1.0 / N) * v[0];

@@ -59,6 +59,10 @@ struct RKJob {
     // (null: a separate pass splits the snapshots)
     void *bf_hi, *bf_lo;
     int bf_kp;
+    // cluster kernel: per-CTA partial sums of the records' autocorrelation,
+    // [W][n_rec][CS], summed into qss by a later launch (null: the cluster
+    // reduces them itself with a cluster barrier per record)
+    double *qpart;
 };
 
 // status bits (1 << k): zero correction denominator; bounded waits that
