@@ -114,7 +114,7 @@ def load():
     L.smd_serve_shutdown.argtypes = [vp]
     L.smd_serve_shutdown.restype = None
     L.smd_evolve_fp64_noalloc.argtypes = [C.POINTER(NoAllocModel), C.c_int, C.c_double, C.c_int,
-                                          vp, vp, vp]
+                                          vp, vp, vp, vp]
     L.smd_measure_fma_peak.argtypes = [C.c_int, C.c_int, dp]
     _lib = L
     return L

@@ -16,6 +16,8 @@
 
 #include "fft_device.cuh"
 
+#include <cstdlib>
+
 namespace smd {
 
 // ---------------------------------------------------------- list projection
@@ -284,13 +286,15 @@ __host__ __device__ inline int p2_table_size(int log2n)
 // (nseq sequences); blockDim.x = nseq * n / 16.  One bulk copy per sample
 // brings the tile; the copy of sample s + 1 is issued as soon as the first
 // pass of sample s has read S, so it overlaps the remaining passes.  The
-// wait on the copy is bounded: on expiry thread 0 records bit 8 in *status,
-// the block stops, and the copy in flight is waited for (bounded) before
-// the block exits.
+// wait on the copy is bounded by poll_limit polls: on expiry thread 0
+// records bit 8 in *status, the block stops, and the copy in flight is
+// waited for (with the fixed limit kDrainPolls) before the block exits.
+constexpr unsigned kDrainPolls = 1u << 26;   // about a second of polling
+
 template <typename T>
 __global__ void __launch_bounds__(sizeof(T) == 8 ? 256 : 512) time_fft_pow2_kernel(
     const cplx<T> *__restrict__ series, int W, int Q, int nqb, int n, int log2n, int nseq,
-    const cplx<T> *__restrict__ tw_g, double *__restrict__ acc, int *status)
+    const cplx<T> *__restrict__ tw_g, double *__restrict__ acc, int *status, unsigned poll_limit)
 {
     constexpr int QB = series_qb<T>();
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -363,7 +367,7 @@ __global__ void __launch_bounds__(sizeof(T) == 8 ? 256 : 512) time_fft_pow2_kern
         // observe the completed phase themselves
         if (threadIdx.x == 0) {
             bool done = false;
-            for (unsigned it = 0; it < (1u << 26) && !done; it++) done = try_wait(s & 1);
+            for (unsigned it = 0; it < poll_limit && !done; it++) done = try_wait(s & 1);
             if (!done) {
                 atomicOr(status, 8);
                 abort_flag = 1;
@@ -429,7 +433,7 @@ __global__ void __launch_bounds__(sizeof(T) == 8 ? 256 : 512) time_fft_pow2_kern
     if (abort_flag) {
         // the copy in flight (sample s_abort) lands before the block exits
         if (threadIdx.x == 0)
-            for (unsigned it = 0; it < (1u << 26) && !try_wait(s_abort & 1); it++) {
+            for (unsigned it = 0; it < kDrainPolls && !try_wait(s_abort & 1); it++) {
             }
         return;
     }
@@ -585,6 +589,10 @@ cudaError_t launch_time_fft(const void *series, int precision, int W, int Q, int
     const int qb = series_qblock(precision);
     const int l2 = pow2_log2(n);
     if (l2 >= 0) {
+        // polls of the bounded copy wait (SMD_TFFT_POLL_LIMIT overrides the
+        // default; a test sets 0 to make the wait expire)
+        unsigned polls = kDrainPolls;
+        if (const char *e = std::getenv("SMD_TFFT_POLL_LIMIT")) polls = (unsigned)std::strtoul(e, nullptr, 10);
         const int nseq = pow2_nseq(n, precision, Q);
         const size_t smem = pow2_smem(n, nseq, precision);
         const int threads = nseq * n / 16;
@@ -593,12 +601,12 @@ cudaError_t launch_time_fft(const void *series, int precision, int W, int Q, int
             auto k = time_fft_pow2_kernel<double>;
             allow_dynamic_smem(k);
             k<<<ncomp * ntile, threads, smem, st>>>((const cplx<double> *)series, W, Q, nqb, n, l2, nseq,
-                                                (const cplx<double> *)tw, acc, status);
+                                                (const cplx<double> *)tw, acc, status, polls);
         } else {
             auto k = time_fft_pow2_kernel<float>;
             allow_dynamic_smem(k);
             k<<<ncomp * ntile, threads, smem, st>>>((const cplx<float> *)series, W, Q, nqb, n, l2, nseq,
-                                                (const cplx<float> *)tw, acc, status);
+                                                (const cplx<float> *)tw, acc, status, polls);
         }
         return cudaGetLastError();
     }

@@ -19,7 +19,6 @@
 // samples into the job's accumulator.
 #include "../../include/smd_b200.h"
 #include "rk_cluster.cuh"
-#include "rk_rows.cuh"
 #include "smd_launch.h"
 
 #include <cuda_runtime.h>
@@ -85,10 +84,7 @@ struct Lattice {
     std::vector<double> pos;
     std::vector<int> nbr_h[3];      // host copies of the active shells' tables
     std::map<int, std::unique_ptr<ClusterTab>> ctabs;   // keyed by CTAs per sample
-    std::mutex cache_mu;            // guards ctabs and the row-band fields
-    // row-band kernel: stencil geometry (-2 unchecked, -1 not applicable),
-    // cells per side, active shells
-    int rows_geom = -2, side = 0, rows_shells = 0;
+    std::mutex cache_mu;            // guards ctabs
 };
 
 struct QSet {
@@ -576,8 +572,6 @@ struct JobGeom {
     size_t elem, celem;
     ClusterTab *ctab = nullptr;   // cluster kernel partition (null: single-CTA kernel)
     int spt = 0, threads = 0;
-    bool rows = false;            // row-band kernel (takes precedence)
-    RowsParams rp{};
 };
 
 // Partition of lattice L over CS CTAs: contiguous site ranges, halo lists,
@@ -737,114 +731,15 @@ ClusterTab *cluster_tables(Lattice &L, int CS)
 // non-zero couplings) keep the single-CTA kernel.  Otherwise the smallest
 // cluster that puts at least ~85% of the SMs to work is taken, within the
 // shared-memory and register limits; SMD_CLUSTER_CTAS forces a size.
-// Row-band kernel eligibility (rk_rows.cuh): one site per cell
-// (N = side^2, site g = x + side y) and, for every active shell, each
-// site's neighbours at exactly the cell offsets of the square or the
-// triangular stencil.
-void rows_check(Lattice &L)
-{
-    std::lock_guard<std::mutex> lk(L.cache_mu);
-    if (L.rows_geom != -2) return;
-    L.rows_geom = -1;
-    const int N = L.N;
-    const int side = (int)std::lround(std::sqrt((double)N));
-    if (side * side != N || side < 6) return;
-    int shells = 0;
-    for (int s = 0; s < 3; s++)
-        if (!L.nbr_h[s].empty() && L.zn[s] > 0) shells |= 1 << s;
-    if (!(shells & 1)) return;
-    for (int geom : {(int)kStencilSquare, (int)kStencilTriang}) {
-        bool ok = true;
-        for (int s = 0; s < 3 && ok; s++) {
-            if (!((shells >> s) & 1)) continue;
-            const int z = L.zn[s];
-            if (z != stencil_z(geom, s)) {
-                ok = false;
-                break;
-            }
-            std::vector<std::pair<int, int>> want(z), got(z);
-            for (int e = 0; e < z; e++) want[e] = {stencil_off(geom, s, e, 0), stencil_off(geom, s, e, 1)};
-            std::sort(want.begin(), want.end());
-            auto wrap = [&](int d) {
-                d = ((d % side) + side) % side;
-                return d >= side / 2 ? d - side : d;
-            };
-            for (int i = 0; i < N && ok; i++) {
-                for (int e = 0; e < z; e++) {
-                    const int j = L.nbr_h[s][(size_t)i * z + e];
-                    if (j < 0 || j >= N) {
-                        ok = false;
-                        break;
-                    }
-                    got[e] = {wrap(j % side - i % side), wrap(j / side - i / side)};
-                }
-                if (!ok) break;
-                std::sort(got.begin(), got.end());
-                ok = got == want;
-            }
-        }
-        if (ok) {
-            L.rows_geom = geom;
-            L.side = side;
-            L.rows_shells = shells;
-            return;
-        }
-    }
-}
-
-// Row bands for the row-band kernel: the smallest band count whose blocks
-// fit the kernel and whose samples x bands fill the SMs (else the largest
-// that fits).  False when the lattice or the form does not fit.
-bool choose_rows(smd_ctx *ctx, JobGeom &g, int n_samples, int sms, int forced)
-{
-    Lattice &L = *g.L;
-    // opt-in (SMD_RK_KERNEL=rows): on the C2 lattice it measured level with
-    // the cluster kernel, which stays the default
-    const char *ke = std::getenv("SMD_RK_KERNEL");
-    if (!(ke && std::strcmp(ke, "rows") == 0)) return false;
-    rows_check(L);
-    if (L.rows_geom < 0 || L.side % rows_spt(g.prec)) return false;
-    bool found = false;
-    for (int CS : {1, 2, 4, 8, 16}) {
-        if (forced && CS != forced) continue;
-        if (L.side / CS < 2) break;
-        RowsParams P{};
-        P.N = L.N;
-        P.L = L.side;
-        P.CS = CS;
-        P.ny_max = 0;
-        for (int r = 0; r <= CS; r++) P.row0[r] = (int)((long long)L.side * r / CS);
-        for (int r = 0; r < CS; r++) P.ny_max = std::max(P.ny_max, P.row0[r + 1] - P.row0[r]);
-        P.geom = L.rows_geom;
-        P.shells = L.rows_shells;
-        P.h = L.dev.h;
-        for (int s = 0; s < 3; s++)
-            for (int c = 0; c < 3; c++) {
-                const bool on = (L.rows_shells >> s) & 1;
-                P.coef64[s][c] = on ? L.dev.coef[s][c] : 0.0;
-                P.coef32[s][c] = (float)P.coef64[s][c];
-            }
-        if (rk_rows_threads(P, g.prec) > rows_max_threads(g.prec)) continue;
-        if (rk_rows_smem(P, g.prec) > 227 * 1024) continue;
-        g.rows = true;
-        g.rp = P;
-        found = true;
-        if (forced || (long long)n_samples * CS >= (long long)(0.85 * sms)) return true;
-    }
-    return found;
-}
-
 void choose_cluster(smd_ctx *ctx, JobGeom &g, int n_samples)
 {
     Lattice &L = *g.L;
     g.ctab = nullptr;
-    g.rows = false;
     if (!L.dev.energy_from_field || L.lieb_delta || !L.vac_only) return;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
     int forced = 0;
     if (const char *e = std::getenv("SMD_CLUSTER_CTAS")) forced = std::atoi(e);
-    if (choose_rows(ctx, g, n_samples, sms, forced)) return;
     const int sizes[] = {1, 2, 4, 8, 16};
     for (int CS : sizes) {
         if (forced && CS != forced) continue;
@@ -896,7 +791,7 @@ int prepare(smd_ctx *ctx, const smd_job_desc *job, JobGeom &g)
     g.prec = job->precision;
     g.nqb = (g.Q + series_qblock(g.prec) - 1) / series_qblock(g.prec);
     choose_cluster(ctx, g, job->n_samples);
-    if (!g.rows && !g.ctab && g.N > rk_max_sites(g.prec))
+    if (!g.ctab && g.N > rk_max_sites(g.prec))
         return fail(ctx, SMD_EINVAL, "job: N exceeds the single-CTA capacity of this form");
     if (g.Qs->use_grid && g.prec == SMD_FP64 && !g.Qs->fp64_ok)
         return fail(ctx, SMD_EINVAL, "job: grid too large for the FP64 shared-memory transform");
@@ -950,7 +845,7 @@ int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const do
         CK(ctx->snap[b].ensure((size_t)W * R * 3 * N * g.elem), "cudaMalloc snap");
     CK(ctx->series.ensure((size_t)W * 3 * n_rec * nqb * 16), "cudaMalloc series");
     CK(ctx->qss.ensure((size_t)W * n_rec * sizeof(double)), "cudaMalloc qss");
-    if (g.ctab && !g.rows)
+    if (g.ctab)
         CK(ctx->qpart.ensure((size_t)W * n_rec * g.ctab->P.CS * sizeof(double)), "cudaMalloc qpart");
     CK(ctx->stats.ensure((size_t)W * 4 * sizeof(double)), "cudaMalloc stats");
     CK(ctx->e0.ensure((size_t)W * sizeof(double)), "cudaMalloc e0");
@@ -1015,10 +910,10 @@ int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const do
             J.qss = ctx->qss.as<double>();
             J.stats = ctx->stats.as<double>();
             J.status = ctx->status.as<int>();
-            J.qpart = (g.ctab && !g.rows) ? ctx->qpart.as<double>() : nullptr;
+            J.qpart = g.ctab ? ctx->qpart.as<double>() : nullptr;
             // the cluster kernel writes the tensor-core operand rows itself
             const bool tc_list = Qs.n_list > 0 && g.prec == SMD_FP32;
-            const bool fused_split = tc_list && g.ctab && !g.rows;
+            const bool fused_split = tc_list && g.ctab;
             if (tc_list) {
                 const int rows = Ww * R * 3, kp = Qs.kp;
                 const size_t ab = (size_t)W * R * 3 * kp * 2;
@@ -1042,9 +937,7 @@ int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const do
             J.bf_lo = fused_split ? ctx->alo[b].p : nullptr;
             J.bf_kp = Qs.kp;
             CK(cudaEventRecord(ev(2 + 2 * c), ctx->s_rk), "event");
-            if (g.rows)
-                CK(launch_rk_rows(g.rp, J, g.prec, ctx->s_rk), "rk row-band kernel");
-            else if (g.ctab) {
+            if (g.ctab) {
                 // SMD_RK_HALO=barrier publishes halos with cluster barriers
                 ClusterParams cp = g.ctab->P;
                 if (const char *e = std::getenv("SMD_RK_HALO"))
@@ -1132,7 +1025,7 @@ int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const do
             ctx->launches++;
         }
         CK(cudaStreamWaitEvent(ctx->s_proj, ctx->ev_rk[(nchunks - 1) % kSnapBufs], 0), "wait");
-        if (g.ctab && !g.rows) {
+        if (g.ctab) {
             CK(launch_qss_from_parts(ctx->qpart.as<double>(), Ww, n_rec, g.ctab->P.CS, N, ctx->qss.as<double>(),
                                      ctx->s_proj),
                "qss");
@@ -1174,8 +1067,8 @@ int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const do
         rep->ms_proj = ms_proj;
         rep->ms_tfft = ms_tfft;
         rep->rk_launches = rk_launches;
-        rep->rk_kind = g.rows ? 2 : g.ctab ? 1 : 0;
-        rep->rk_ctas = g.rows ? g.rp.CS : g.ctab ? g.ctab->P.CS : 1;
+        rep->rk_kind = g.ctab ? 1 : 0;
+        rep->rk_ctas = g.ctab ? g.ctab->P.CS : 1;
         rep->site_steps = (double)N * (double)(n_rec - 1) * job->stride * job->n_samples;
     }
     if (st & 4) return fail(ctx, SMD_ETIMEOUT, "tensor-core projection: a bounded wait expired");

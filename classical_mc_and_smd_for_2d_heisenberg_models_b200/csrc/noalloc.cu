@@ -51,7 +51,7 @@ size_t scratch_bytes(long long S, long long N)
 
 extern "C" int smd_evolve_fp64_noalloc(const smd_noalloc_model *m, int n_samples, double dt,
                                        int nsteps, const double *d_spins_in, double *d_spins_out,
-                                       void *stream)
+                                       int *d_status, void *stream)
 {
     if (!m || !m->d_nbr || !d_spins_in || !d_spins_out) return SMD_EINVAL;
     if (m->N <= 0 || n_samples <= 0 || nsteps < 1 || !(dt > 0.0)) return SMD_EINVAL;
@@ -85,9 +85,9 @@ extern "C" int smd_evolve_fp64_noalloc(const smd_noalloc_model *m, int n_samples
     double *qss = reinterpret_cast<double *>(q);    q += up256(S * 2 * 8);
     double *stats = reinterpret_cast<double *>(q);  q += up256(S * 4 * 8);
     double *e0 = reinterpret_cast<double *>(q);     q += up256(S * 8);
-    int *status = reinterpret_cast<int *>(q);
-
-    // the status word is the only scratch read before it is written
+    // the kernel's status bits go to the caller's word when one is given,
+    // else to the array's; it is the only word read before it is written
+    int *status = d_status ? d_status : reinterpret_cast<int *>(q);
     if (cudaMemsetAsync(status, 0, sizeof(int), st) != cudaSuccess) return SMD_ECUDA;
 
     LatticeDev L{};

@@ -13,7 +13,7 @@ size_t rk_cluster_smem(const ClusterParams &P, int precision)
     const size_t Np = (size_t)P.n_loc_max + 1;
     size_t b = 2 * Np * v4 + (size_t)(P.ZT / 2) * P.n_own_max * 4 + (size_t)P.pmax * P.n_own_max * 4;
     b = (b + 15) & ~size_t(15);
-    b += 2 * kMaxClusterCTAs * 4 * sizeof(double) + 32 * 4 * sizeof(double) + 2 * sizeof(uint64_t);
+    b += 2 * kMaxClusterCTAs * 8 * sizeof(double) + 32 * 8 * sizeof(double) + 2 * sizeof(uint64_t);
     // FP32 form: FP64 master spins of the own sites
     return b + (precision == 0 ? 0 : (size_t)3 * P.n_own_max * sizeof(double));
 }

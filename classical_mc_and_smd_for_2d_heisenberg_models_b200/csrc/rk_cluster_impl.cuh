@@ -111,9 +111,9 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
     int *push = reinterpret_cast<int *>(idx + (ZT / 2) * nom);
     size_t off = (size_t)(reinterpret_cast<unsigned char *>(push + P.pmax * nom) - smem_raw);
     off = (off + 15) & ~size_t(15);
-    double *red = reinterpret_cast<double *>(smem_raw + off);   // [2][16][4]
-    double *wpart = red + 2 * kMaxClusterCTAs * 4;                // [32][4]
-    uint64_t *hbar = reinterpret_cast<uint64_t *>(wpart + 32 * 4);  // [2] halo publish barriers
+    double *red = reinterpret_cast<double *>(smem_raw + off);   // [2][16][4][2] compensated partials
+    double *wpart = red + 2 * kMaxClusterCTAs * 8;                // [32][4][2]
+    uint64_t *hbar = reinterpret_cast<uint64_t *>(wpart + 32 * 8);  // [2] halo publish barriers
     double *Sm = reinterpret_cast<double *>(hbar + 2);              // [3][nom], FP32 form only
     double *D = reinterpret_cast<double *>(smem_raw);             // [3][Np], FP32 form only
 
@@ -235,31 +235,39 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
         else wait();
     };
 
-    // Sum of NV doubles over every thread of every CTA of the cluster; all
-    // threads receive the totals, summed in a fixed order.
-    auto cluster_sum = [&](double *v, int NV) {
+    // Compensated sum (csum) of NV values over every thread of every CTA of
+    // the cluster; all threads receive the totals, summed in a fixed order.
+    auto cluster_sum = [&](csum *v, int NV) {
         const int lane = tid & 31, warp = tid >> 5, nw = (NT + 31) >> 5;
-        for (int q = 0; q < NV; q++) v[q] = warp_sum(v[q]);
+        for (int q = 0; q < NV; q++) v[q] = warp_sum_c(v[q]);
         if (lane == 0)
-            for (int q = 0; q < NV; q++) wpart[warp * 4 + q] = v[q];
+            for (int q = 0; q < NV; q++) {
+                wpart[(warp * 4 + q) * 2] = v[q].s;
+                wpart[(warp * 4 + q) * 2 + 1] = v[q].c;
+            }
         __syncthreads();
         if (warp == 0) {
             for (int q = 0; q < NV; q++) {
-                double x = (lane < nw) ? wpart[lane * 4 + q] : 0.0;
-                x = warp_sum(x);
+                csum x = (lane < nw) ? csum{wpart[(lane * 4 + q) * 2], wpart[(lane * 4 + q) * 2 + 1]}
+                                     : csum{0.0, 0.0};
+                x = warp_sum_c(x);
                 if (lane == 0) {
                     for (int r = 0; r < CS; r++) {
-                        double *rr = cl.map_shared_rank(red, r);
-                        rr[slot * kMaxClusterCTAs * 4 + rank * 4 + q] = x;
+                        double *rr = cl.map_shared_rank(red, r) + ((slot * kMaxClusterCTAs + rank) * 4 + q) * 2;
+                        rr[0] = x.s;
+                        rr[1] = x.c;
                     }
                 }
             }
         }
         cl.sync();
         for (int q = 0; q < NV; q++) {
-            double s = 0.0;
-            for (int r = 0; r < CS; r++) s += red[slot * kMaxClusterCTAs * 4 + r * 4 + q];
-            v[q] = s;
+            csum t{0.0, 0.0};
+            for (int r = 0; r < CS; r++) {
+                const double *rr = red + ((slot * kMaxClusterCTAs + r) * 4 + q) * 2;
+                t = csum_add(t, csum{rr[0], rr[1]});
+            }
+            v[q] = t;
         }
         slot ^= 1;
     };
@@ -394,7 +402,7 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
     // FP64 energy of the state S (A holds it in the FP64 form; the FP32 form
     // fills D from the owners first).  Call after a cluster barrier.
     auto energy = [&]() -> double {
-        double e = 0.0;
+        csum e{0.0, 0.0};
 #pragma unroll
         for (int k = 0; k < SPT; k++) {
             const int li = tid + k * NT;
@@ -407,12 +415,12 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
                 } else {
                     field64(k, li, (double)mk[k], h);
                 }
-                e += S[k][0] * h[0] + S[k][1] * h[1] + S[k][2] * h[2] - hz * S[k][2];
+                csum_acc(e, S[k][0] * h[0] + S[k][1] * h[1] + S[k][2] * h[2] - hz * S[k][2]);
             }
         }
-        double v[1] = {e};
+        csum v[1] = {e};
         cluster_sum(v, 1);
-        return 0.5 * v[0];
+        return 0.5 * csum_val(v[0]);
     };
     auto publishD = [&]() {
 #pragma unroll
@@ -475,18 +483,18 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
             // no cluster barrier at a record
             const int lane = tid & 31, warp = tid >> 5, nw = (NT + 31) >> 5;
             const double x = warp_sum(p);
-            if (lane == 0) wpart[warp * 4] = x;
+            if (lane == 0) wpart[warp * 8] = x;
             __syncthreads();
             if (warp == 0) {
-                const double y = warp_sum((lane < nw) ? wpart[lane * 4] : 0.0);
+                const double y = warp_sum((lane < nw) ? wpart[lane * 8] : 0.0);
                 if (lane == 0) J.qpart[((size_t)smp * J.n_rec + r) * CS + rank] = y;
             }
             __syncthreads();   // wpart is read before the next reduction writes it
             return;
         }
-        double v[1] = {p};
+        csum v[1] = {csum{p, 0.0}};
         cluster_sum(v, 1);
-        if (rank == 0 && tid == 0) J.qss[(size_t)smp * J.n_rec + r] = (r == 0) ? 1.0 : (1.0 / N) * v[0];
+        if (rank == 0 && tid == 0) J.qss[(size_t)smp * J.n_rec + r] = (r == 0) ? 1.0 : (1.0 / N) * csum_val(v[0]);
     };
 
     if (AH && tid == 0) {
@@ -555,7 +563,7 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
         for (int ss = 0; ss < J.stride; ss++) {
             const int n = (r - 1) * J.stride + ss + 1;
             const bool fix = per_step || (n % F == 0);
-            double eref = 0.0;
+            csum eref{0.0, 0.0};
             // ---- stage 1: A -> B
             begin_pub();
             two_pass([&](int k) {
@@ -566,7 +574,7 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
                 Sp[1] = spin(k, 1);
                 Sp[2] = spin(k, 2);
                 if (sizeof(T) == 8 && per_step)
-                    eref += S[k][0] * h[0] + S[k][1] * h[1] + S[k][2] * h[2] - hz * S[k][2];
+                    csum_acc(eref, S[k][0] * h[0] + S[k][1] * h[1] + S[k][2] * h[2] - hz * S[k][2]);
                 Pv[0] = h[1] * Sp[2] - h[2] * Sp[1];
                 Pv[1] = h[2] * Sp[0] - h[0] * Sp[2];
                 Pv[2] = h[0] * Sp[1] - h[1] * Sp[0];
@@ -649,7 +657,7 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
                 publishA();
                 cl_sync();
             }
-            double sig = 0.0, e1 = 0.0;
+            csum sig{0.0, 0.0}, e1{0.0, 0.0};
 #pragma unroll
             for (int k = 0; k < SPT; k++) {
                 const int li = tid + k * NT;
@@ -665,14 +673,15 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
                     Pv[0] = h[1] * S[k][2] - h[2] * S[k][1];
                     Pv[1] = h[2] * S[k][0] - h[0] * S[k][2];
                     Pv[2] = h[0] * S[k][1] - h[1] * S[k][0];
-                    sig += Pv[0] * Pv[0] + Pv[1] * Pv[1] + Pv[2] * Pv[2];
-                    e1 += S[k][0] * h[0] + S[k][1] * h[1] + S[k][2] * h[2] - hz * S[k][2];
+                    csum_acc(sig, Pv[0] * Pv[0] + Pv[1] * Pv[1] + Pv[2] * Pv[2]);
+                    csum_acc(e1, S[k][0] * h[0] + S[k][1] * h[1] + S[k][2] * h[2] - hz * S[k][2]);
 #pragma unroll
                     for (int c = 0; c < 3; c++) acc[k][c] = T(Pv[c]);
                 }
             }
-            double v3[3] = {eref, sig, e1};
-            cluster_sum(v3, 3);
+            csum t3[3] = {eref, sig, e1};
+            cluster_sum(t3, 3);
+            const double v3[3] = {csum_val(t3[0]), csum_val(t3[1]), csum_val(t3[2])};
             const double Eref = (sizeof(T) == 8 && per_step) ? 0.5 * v3[0] : E0;
             const double E1 = 0.5 * v3[2];
             double scale = (Eref - E1) / v3[1];

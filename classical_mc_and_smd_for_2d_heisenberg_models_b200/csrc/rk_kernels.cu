@@ -162,22 +162,22 @@ __device__ __forceinline__ void normalise3(double v[3])
 }
 
 // Bond-list energy for lattices where the field identity does not hold;
-// returns this thread's partial sum.  b is an FP64 SoA field.
-__device__ double energy_bonds(const LatticeDev &L, const double *b, int N,
-                               const uint8_t *imp)
+// returns this thread's compensated partial sum.  b is an FP64 SoA field.
+__device__ csum energy_bonds(const LatticeDev &L, const double *b, int N,
+                             const uint8_t *imp)
 {
-    double e = 0.0;
+    csum e{0.0, 0.0};
     for (int q = threadIdx.x; q < L.nbonds; q += blockDim.x) {
         const int4 bd = L.bonds[q];
         const int i = bd.x, j = bd.y, s = bd.z;
         double Jv = imp ? L.J[s][imp[i]][imp[j]] : L.J[s][0][0];
         if (s == 1 && L.lieb_delta_on)
             Jv += ((i & 1) ? -1 : 1) * ((j & 1) ? -1 : 1) * L.j2_delta;
-        e += Jv * L.lam[s][0] * b[i] * b[j] + Jv * L.lam[s][1] * b[N + i] * b[N + j] +
-             Jv * L.lam[s][2] * b[2 * N + i] * b[2 * N + j];
+        csum_acc(e, Jv * L.lam[s][0] * b[i] * b[j] + Jv * L.lam[s][1] * b[N + i] * b[N + j] +
+                        Jv * L.lam[s][2] * b[2 * N + i] * b[2 * N + j]);
     }
     if (L.h != 0.0)
-        for (int i = threadIdx.x; i < N; i += blockDim.x) e += (-L.h) * b[2 * N + i];
+        for (int i = threadIdx.x; i < N; i += blockDim.x) csum_acc(e, (-L.h) * b[2 * N + i]);
     return e;
 }
 
@@ -192,7 +192,7 @@ __device__ __forceinline__ void carve(unsigned char *raw, int N, T *&A, T *&B, d
     size_t off = (size_t)6 * N * sizeof(T);
     off = (off + 15) & ~size_t(15);
     red = reinterpret_cast<double *>(raw + off);
-    imp_s = reinterpret_cast<uint8_t *>(red + 2 * 32 * 4);
+    imp_s = reinterpret_cast<uint8_t *>(red + 2 * 32 * 8);
 }
 
 // ------------------------------------------------------------------ FP64
@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(rk_maxt(0, MAXSPT), 1) rk_fp64_kernel(const La
 
     // energy of the state held in A and S (call after a barrier)
     auto energy_of_A = [&]() -> double {
-        double e = 0.0;
+        csum e{0.0, 0.0};
         if (efield) {
 #pragma unroll
             for (int k = 0; k < MAXSPT; k++) {
@@ -255,15 +255,15 @@ __global__ void __launch_bounds__(rk_maxt(0, MAXSPT), 1) rk_fp64_kernel(const La
                 if (i < N) {
                     double h[3];
                     local_field<double, GEN>(L, A, N, i, ai[k], imp, h);
-                    e += S[k][0] * h[0] + S[k][1] * h[1] + S[k][2] * h[2] - hz * S[k][2];
+                    csum_acc(e, S[k][0] * h[0] + S[k][1] * h[1] + S[k][2] * h[2] - hz * S[k][2]);
                 }
             }
         } else {
             e = energy_bonds(L, A, N, imp);
         }
-        double v[1] = {e};
-        block_sum<1>(v, red, slot);
-        return efield ? 0.5 * v[0] : v[0];
+        csum v[1] = {e};
+        block_sum_c<1>(v, red, slot);
+        return efield ? 0.5 * csum_val(v[0]) : csum_val(v[0]);
     };
     auto record = [&](int r) {
         const size_t base = ((size_t)smp * J.snap_R + (r - J.rec_begin)) * 3 * N;
@@ -279,9 +279,9 @@ __global__ void __launch_bounds__(rk_maxt(0, MAXSPT), 1) rk_fp64_kernel(const La
                 }
             }
         }
-        double v[1] = {p};
-        block_sum<1>(v, red, slot);
-        if (tid == 0) J.qss[(size_t)smp * J.n_rec + r] = (r == 0) ? 1.0 : (1.0 / N) * v[0];
+        csum v[1] = {csum{p, 0.0}};
+        block_sum_c<1>(v, red, slot);
+        if (tid == 0) J.qss[(size_t)smp * J.n_rec + r] = (r == 0) ? 1.0 : (1.0 / N) * csum_val(v[0]);
     };
 
     double E0;
@@ -303,7 +303,7 @@ __global__ void __launch_bounds__(rk_maxt(0, MAXSPT), 1) rk_fp64_kernel(const La
             const int n = (r - 1) * J.stride + ss + 1;
             const bool fix = per_step || (n % J.fix_every == 0);
             double acc[MAXSPT][3];
-            double eref = 0.0;
+            csum eref{0.0, 0.0};
             // ---- stage 1: A -> B
 #pragma unroll
             for (int k = 0; k < MAXSPT; k++) {
@@ -312,7 +312,7 @@ __global__ void __launch_bounds__(rk_maxt(0, MAXSPT), 1) rk_fp64_kernel(const La
                     double h[3], P[3];
                     local_field<double, GEN>(L, A, N, i, ai[k], imp, h);
                     if (per_step && efield)
-                        eref += S[k][0] * h[0] + S[k][1] * h[1] + S[k][2] * h[2] - hz * S[k][2];
+                        csum_acc(eref, S[k][0] * h[0] + S[k][1] * h[1] + S[k][2] * h[2] - hz * S[k][2]);
                     cross3(h, S[k], P);
 #pragma unroll
                     for (int c = 0; c < 3; c++) {
@@ -378,7 +378,7 @@ __global__ void __launch_bounds__(rk_maxt(0, MAXSPT), 1) rk_fp64_kernel(const La
             __syncthreads();
             if (!fix) continue;
             // ---- energy correction: sigma sweep on A, P kept in acc
-            double sig = 0.0, e1 = 0.0;
+            csum sig{0.0, 0.0}, e1{0.0, 0.0};
 #pragma unroll
             for (int k = 0; k < MAXSPT; k++) {
                 const int i = tid + k * T;
@@ -386,16 +386,17 @@ __global__ void __launch_bounds__(rk_maxt(0, MAXSPT), 1) rk_fp64_kernel(const La
                     double h[3], P[3];
                     local_field<double, GEN>(L, A, N, i, ai[k], imp, h);
                     cross3(h, S[k], P);
-                    sig += P[0] * P[0] + P[1] * P[1] + P[2] * P[2];
+                    csum_acc(sig, P[0] * P[0] + P[1] * P[1] + P[2] * P[2]);
                     if (efield)
-                        e1 += S[k][0] * h[0] + S[k][1] * h[1] + S[k][2] * h[2] - hz * S[k][2];
+                        csum_acc(e1, S[k][0] * h[0] + S[k][1] * h[1] + S[k][2] * h[2] - hz * S[k][2]);
 #pragma unroll
                     for (int c = 0; c < 3; c++) acc[k][c] = P[c];
                 }
             }
             if (!efield) e1 = energy_bonds(L, A, N, imp);
-            double v3[3] = {eref, sig, e1};
-            block_sum<3>(v3, red, slot);
+            csum t3[3] = {eref, sig, e1};
+            block_sum_c<3>(t3, red, slot);
+            const double v3[3] = {csum_val(t3[0]), csum_val(t3[1]), csum_val(t3[2])};
             const double Eref = per_step ? (efield ? 0.5 * v3[0] : v3[0]) : E0;
             const double E1 = efield ? 0.5 * v3[2] : v3[2];
             double scale = (Eref - E1) / v3[1];
@@ -541,7 +542,7 @@ __global__ void __launch_bounds__(rk_maxt(1, MAXSPT), 1) rk_fp32_kernel(const La
     };
     // FP64 energy of S (D must hold S; call after a barrier)
     auto energy_of_D = [&]() -> double {
-        double e = 0.0;
+        csum e{0.0, 0.0};
         if (efield) {
 #pragma unroll
             for (int k = 0; k < MAXSPT; k++) {
@@ -549,15 +550,15 @@ __global__ void __launch_bounds__(rk_maxt(1, MAXSPT), 1) rk_fp32_kernel(const La
                 if (i < N) {
                     double h[3];
                     local_field<double, GEN>(L, D, N, i, ai[k], imp, h);
-                    e += S[k][0] * h[0] + S[k][1] * h[1] + S[k][2] * h[2] - hz * S[k][2];
+                    csum_acc(e, S[k][0] * h[0] + S[k][1] * h[1] + S[k][2] * h[2] - hz * S[k][2]);
                 }
             }
         } else {
             e = energy_bonds(L, D, N, imp);
         }
-        double v[1] = {e};
-        block_sum<1>(v, red, slot);
-        return efield ? 0.5 * v[0] : v[0];
+        csum v[1] = {e};
+        block_sum_c<1>(v, red, slot);
+        return efield ? 0.5 * csum_val(v[0]) : csum_val(v[0]);
     };
     auto record = [&](int r) {
         const size_t base = ((size_t)smp * J.snap_R + (r - J.rec_begin)) * 3 * N;
@@ -573,9 +574,9 @@ __global__ void __launch_bounds__(rk_maxt(1, MAXSPT), 1) rk_fp32_kernel(const La
                 }
             }
         }
-        double v[1] = {p};
-        block_sum<1>(v, red, slot);
-        if (tid == 0) J.qss[(size_t)smp * J.n_rec + r] = (r == 0) ? 1.0 : (1.0 / N) * v[0];
+        csum v[1] = {csum{p, 0.0}};
+        block_sum_c<1>(v, red, slot);
+        if (tid == 0) J.qss[(size_t)smp * J.n_rec + r] = (r == 0) ? 1.0 : (1.0 / N) * csum_val(v[0]);
     };
 
     double E0;
@@ -679,7 +680,7 @@ __global__ void __launch_bounds__(rk_maxt(1, MAXSPT), 1) rk_fp32_kernel(const La
             // ---- FP64 energy correction against E0
             store_D();
             __syncthreads();
-            double sig = 0.0, e1 = 0.0;
+            csum sig{0.0, 0.0}, e1{0.0, 0.0};
 #pragma unroll
             for (int k = 0; k < MAXSPT; k++) {
                 const int i = tid + k * T;
@@ -687,16 +688,17 @@ __global__ void __launch_bounds__(rk_maxt(1, MAXSPT), 1) rk_fp32_kernel(const La
                     double h[3], P[3];
                     local_field<double, GEN>(L, D, N, i, ai[k], imp, h);
                     cross3(h, S[k], P);
-                    sig += P[0] * P[0] + P[1] * P[1] + P[2] * P[2];
+                    csum_acc(sig, P[0] * P[0] + P[1] * P[1] + P[2] * P[2]);
                     if (efield)
-                        e1 += S[k][0] * h[0] + S[k][1] * h[1] + S[k][2] * h[2] - hz * S[k][2];
+                        csum_acc(e1, S[k][0] * h[0] + S[k][1] * h[1] + S[k][2] * h[2] - hz * S[k][2]);
 #pragma unroll
                     for (int c = 0; c < 3; c++) acc[k][c] = (float)P[c];
                 }
             }
             if (!efield) e1 = energy_bonds(L, D, N, imp);
-            double v2[2] = {sig, e1};
-            block_sum<2>(v2, red, slot);
+            csum t2[2] = {sig, e1};
+            block_sum_c<2>(t2, red, slot);
+            const double v2[2] = {csum_val(t2[0]), csum_val(t2[1])};
             const double E1 = efield ? 0.5 * v2[1] : v2[1];
             double scale = (E0 - E1) / v2[0];
             if (!(v2[0] > 0.0)) {
@@ -755,7 +757,7 @@ size_t rk_smem_bytes(int N, int precision)
     const size_t elem = precision == 0 ? sizeof(double) : sizeof(float);
     size_t off = (size_t)6 * N * elem;
     off = (off + 15) & ~size_t(15);
-    return off + 2 * 32 * 4 * sizeof(double) + (size_t)N;
+    return off + 2 * 32 * 8 * sizeof(double) + (size_t)N;
 }
 
 template <int MAXSPT, bool GEN>

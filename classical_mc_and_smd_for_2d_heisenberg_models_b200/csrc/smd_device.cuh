@@ -126,6 +126,65 @@ __device__ __forceinline__ double warp_sum(double v)
     return v;
 }
 
+// Compensated sum (Neumaier): the value is s + c, where c collects the exact
+// rounding error of every addition into s (Knuth's TwoSum, exact for any
+// operand order), so a sum of many terms carries about twice the working
+// precision.  Used for the per-sample energies and the correction's sigma
+// (Codes_Folder/subrouts.cpp:5181-5302, 11862-11902), whose difference
+// E_ref - E1 sets the correction scale.  csum_add(a, b) and csum_add(b, a)
+// are bit-identical, so butterfly (xor) shuffles leave every lane with the
+// same total.
+struct csum {
+    double s, c;
+};
+
+__device__ __forceinline__ csum csum_add(csum a, csum b)
+{
+    const double s = a.s + b.s;
+    const double bp = s - a.s;
+    const double e = (a.s - (s - bp)) + (b.s - bp);
+    return {s, (a.c + b.c) + e};
+}
+
+__device__ __forceinline__ void csum_acc(csum &a, double x) { a = csum_add(a, csum{x, 0.0}); }
+
+__device__ __forceinline__ double csum_val(csum a) { return a.s + a.c; }
+
+__device__ __forceinline__ csum warp_sum_c(csum v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        v = csum_add(v, csum{__shfl_xor_sync(0xffffffffu, v.s, o), __shfl_xor_sync(0xffffffffu, v.c, o)});
+    return v;
+}
+
+// Block-wide compensated sum of NV values; every thread receives the totals
+// (s + c).  red holds two slots of [32][NV][2] doubles (NV <= 4); the order
+// of the additions is fixed, so results are deterministic run to run.
+template <int NV>
+__device__ __forceinline__ void block_sum_c(csum (&v)[NV], double *red, int &slot)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; k++) v[k] = warp_sum_c(v[k]);
+    double *r = red + slot * 32 * 8;
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+            r[(warp * NV + k) * 2] = v[k].s;
+            r[(warp * NV + k) * 2 + 1] = v[k].c;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+        csum x = (lane < nw) ? csum{r[(lane * NV + k) * 2], r[(lane * NV + k) * 2 + 1]} : csum{0.0, 0.0};
+        v[k] = warp_sum_c(x);
+    }
+    slot ^= 1;
+}
+
 // Block-wide sum of NV doubles; every thread receives the totals.  red holds
 // two slots of [32][NV]; alternating slots lets consecutive reductions run
 // with a single barrier each.  Summation order is fixed, so results are

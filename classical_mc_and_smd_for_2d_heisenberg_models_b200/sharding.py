@@ -11,7 +11,8 @@ get_dynSpectrum on it, and the root adds every rank's running sums of
 Here a rank is one GPU (one process, torch.distributed).  Samples are
 independent, so there is no exchange during a job; the only collective is
 one sum of the accumulators when the job ends.  ``reduce_sums`` takes any
-process group (NCCL on GPUs, gloo on the host).
+process group: over NCCL the buffer goes to the rank's current GPU for the
+collective, over gloo it stays on the host.
 """
 from __future__ import annotations
 
@@ -49,14 +50,28 @@ def reduce_sums(spec_sum: np.ndarray, qss_sum: np.ndarray, n_local: int,
     qss = torch.from_numpy(np.ascontiguousarray(qss_sum, np.float64))
     cnt = torch.tensor([float(n_local)], dtype=torch.float64)
     flat = torch.cat([spec.reshape(-1), qss.reshape(-1), cnt])
+    flat = flat.to(collective_device(group))
     if dst is None:
         dist.all_reduce(flat, op=dist.ReduceOp.SUM, group=group)
     else:
         dist.reduce(flat, dst=dst, op=dist.ReduceOp.SUM, group=group)
+    flat = flat.cpu()
     n_spec = spec.numel()
     out_spec = flat[:n_spec].reshape(spec.shape).numpy().copy()
     out_qss = flat[n_spec:n_spec + qss.numel()].reshape(qss.shape).numpy().copy()
     return out_spec, out_qss, int(round(float(flat[-1])))
+
+
+def collective_device(group=None):
+    """Where the collective's buffer must live: this rank's current CUDA
+    device for an NCCL group (NCCL takes device tensors only), the host for
+    gloo."""
+    import torch
+    import torch.distributed as dist
+
+    if dist.get_backend(group) == "nccl":
+        return torch.device("cuda", torch.cuda.current_device())
+    return torch.device("cpu")
 
 
 def average(spec_total: np.ndarray, qss_total: np.ndarray, n_total: int):

@@ -165,7 +165,7 @@ typedef struct {
     double ms_proj;        /* summed duration of the projection launches */
     double ms_tfft;        /* summed duration of the time-transform launches */
     int rk_launches;       /* RK kernel launches */
-    int rk_kind;           /* RK kernel used: 0 single-CTA, 1 cluster, 2 row-band */
+    int rk_kind;           /* RK kernel used: 0 single-CTA, 1 cluster */
     int rk_ctas;           /* CTAs per sample (cluster size) */
 } smd_report;
 
@@ -247,6 +247,12 @@ typedef struct {
  * framework's memory pool, or a real-time loop that may not allocate once
  * running) and so cannot let this library call cudaMalloc.
  *   d_spins_in, d_spins_out: DEVICE [n_samples][N][3] (may be the same buffer)
+ *   d_status: DEVICE int owned by the caller, or NULL.  It is set to 0 on the
+ *           stream and then receives the RK kernel's status bits: nonzero
+ *           (bit 1) when a sample met a zero correction denominator, in which
+ *           case that sample's spins are not trustworthy.  Read it once the
+ *           stream has completed; smd_evolve reports the same condition as
+ *           SMD_ECUDA.
  *   stream: cudaStream_t to enqueue on (NULL = default stream); the call
  *           returns once the work is enqueued.
  * Working memory comes from one static device array of
@@ -260,7 +266,7 @@ typedef struct {
  * each direction (true for smd_build_lattice tables with L >= 4). */
 SMD_API int smd_evolve_fp64_noalloc(const smd_noalloc_model *m, int n_samples, double dt,
                                     int nsteps, const double *d_spins_in, double *d_spins_out,
-                                    void *stream);
+                                    int *d_status, void *stream);
 
 /* ---------------------------------------------------------- diagnostics */
 

@@ -99,3 +99,29 @@ def test_two_rank_reduction_equals_single_process(tmp_path, oracle_mod, use_redu
         assert int(d["n"]) == N_SAMPLES
         assert np.allclose(d["spec"], ref_spec, rtol=1e-13, atol=1e-15 * np.abs(ref_spec).max())
         assert np.allclose(d["qss"], ref_qss, rtol=1e-13, atol=1e-15)
+
+
+@pytest.mark.gpu
+def test_run_sharded_over_nccl_one_rank(ctx):
+    """run_sharded over an NCCL process group (one rank: the GPU box has one
+    GPU): the accumulators go through a device-tensor all-reduce and the
+    averages equal the plain run's."""
+    import torch
+    import torch.distributed as dist
+    from classical_mc_and_smd_for_2d_heisenberg_models_b200 import smd
+    s, spins, win = _problem()
+    lat = smd.build_lattice(s.geom, s.L)
+    lid = ctx.lattice(s, lat)
+    qid = ctx.qset(lid)
+    direct = ctx.run(lid, qid, spins, s.dtm, N_REC, stride=2, win=win)
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{_free_port()}", rank=0,
+                            world_size=1)
+    try:
+        assert sharding.collective_device().type == "cuda"
+        spec, qss = sharding.run_sharded(ctx, lid, qid, spins, s.dtm, N_REC, 0, 1, win=win,
+                                         stride=2)
+    finally:
+        dist.destroy_process_group()
+    assert np.allclose(spec, direct.spec, rtol=1e-14, atol=1e-16 * np.abs(direct.spec).max())
+    assert np.allclose(qss, direct.qss, rtol=1e-14, atol=1e-16)
