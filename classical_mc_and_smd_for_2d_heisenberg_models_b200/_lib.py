@@ -26,7 +26,8 @@ EXPORTS = [
     "smd_geometry_info", "smd_build_lattice", "smd_build_bonds", "smd_window",
     "smd_lattice_upload", "smd_lattice_free", "smd_qset_upload", "smd_qset_size",
     "smd_lattice_sites", "smd_run", "smd_run_device", "smd_dyn_spectrum_ref",
-    "smd_evolve", "smd_submit", "smd_poll", "smd_wait", "smd_cancel",
+    "smd_evolve", "smd_batch_create", "smd_batch_info", "smd_batch_run",
+    "smd_batch_run_device", "smd_batch_free", "smd_submit", "smd_poll", "smd_wait", "smd_cancel",
     "smd_serve_shutdown", "smd_evolve_fp64_noalloc", "smd_measure_fma_peak",
 ]
 
@@ -54,6 +55,24 @@ class JobDesc(C.Structure):
     _fields_ = [("lattice", C.c_int), ("qset", C.c_int), ("n_samples", C.c_int),
                 ("dt", C.c_double), ("n_rec", C.c_int), ("stride", C.c_int),
                 ("precision", C.c_int), ("fix_every", C.c_int), ("imp", C.c_void_p)]
+
+
+class BatchMember(C.Structure):
+    _fields_ = [("lattice", C.c_int), ("qset", C.c_int), ("n_samples", C.c_int),
+                ("imp", C.c_void_p)]
+
+
+class BatchDesc(C.Structure):
+    _fields_ = [("n_members", C.c_int), ("members", C.POINTER(BatchMember)), ("dt", C.c_double),
+                ("n_rec", C.c_int), ("stride", C.c_int), ("precision", C.c_int),
+                ("fix_every", C.c_int)]
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [("cluster_ctas", C.c_int), ("sites_per_thread", C.c_int), ("threads", C.c_int),
+                ("edge_slots", C.c_int), ("records_per_launch", C.c_int), ("clusters", C.c_int),
+                ("items", C.c_int), ("candidates", C.c_int), ("probe_ms", C.c_double),
+                ("member_ctas", C.c_int * 24)]
 
 
 class NoAllocModel(C.Structure):
@@ -107,6 +126,13 @@ def load():
                                        dp, dp, dp, dp]
     L.smd_evolve.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, ip,
                              dp, C.POINTER(Report)]
+    L.smd_batch_create.argtypes = [vp, C.POINTER(BatchDesc), ip]
+    L.smd_batch_info.argtypes = [vp, C.c_int, C.POINTER(BatchTuning)]
+    L.smd_batch_run.argtypes = [vp, C.c_int, C.POINTER(dp), dp, C.POINTER(dp), C.POINTER(dp),
+                                C.POINTER(Report)]
+    L.smd_batch_run_device.argtypes = [vp, C.c_int, C.POINTER(vp), vp, C.POINTER(vp),
+                                       C.POINTER(vp), C.POINTER(Report)]
+    L.smd_batch_free.argtypes = [vp, C.c_int]
     L.smd_submit.argtypes = [vp, C.POINTER(JobDesc), dp, dp, dp, dp, C.POINTER(C.c_longlong)]
     L.smd_poll.argtypes = [vp, C.c_longlong, dp]
     L.smd_wait.argtypes = [vp, C.c_longlong, C.c_double, dp]

@@ -1,11 +1,8 @@
-// fft_kernels.cu -- list projection (FP64 form) and the time transform
+// fft_kernels.cu -- the time transform
 // |S(q,w)|^2 accumulated over samples.
 //
-// List q (get_qct_SqData, Codes_Folder/subrouts.cpp:8460-8525): S(q_l) =
-// scale sum_k S_k exp(-i q_l . pos_k), a dense contraction of the snapshot
-// rows with a phase table; the FP64 form runs it as a tiled SIMT GEMM (the
-// FP32 form on the tensor cores, proj_tc.cu).  The grid q are in
-// grid_proj.cu.
+// The list-q projections are in proj_f64.cu (FP64, DMMA) and proj_tc.cu
+// (FP32 form, tcgen05); the grid q in grid_proj.cu.
 //
 // Time transform (Codes_Folder/subrouts.cpp:12062-12109): x[t] = w[t] S(q,t)
 // (the projections store the window-weighted series), forward FFT of length
@@ -19,70 +16,6 @@
 #include <cstdlib>
 
 namespace smd {
-
-// ---------------------------------------------------------- list projection
-
-// Tiled SIMT GEMM: out[m][l] = sum_k A[m][k] P[k][l], A = snapshot rows
-// ([rows][N]), P = phase table ([N][L] complex, scale folded in).
-// 64 rows x 32 complex columns per CTA, 256 threads, 4 x 2 outputs each.
-template <typename T>
-__global__ void __launch_bounds__(256) list_proj_simt_kernel(
-    const T *__restrict__ snap, int rows, int N, int R, int rec_begin,
-    int n_rec_total, const cplx<T> *__restrict__ P, int Lq, const double *__restrict__ win,
-    cplx<T> *__restrict__ series, int nqb, int qoff)
-{
-    constexpr int BM = 64, BL = 32, BK = 16;
-    __shared__ T As[BK][BM + 1];
-    __shared__ cplx<T> Ps[BK][BL];
-    const int m0 = blockIdx.x * BM, l0 = blockIdx.y * BL, s = blockIdx.z;
-    snap += (size_t)s * R * 3 * N;
-    const int tid = threadIdx.x;
-    const int tm = tid / 16, tl = tid % 16;   // 16 x 16 thread grid
-    T ar[4][2][2] = {};
-    for (int k0 = 0; k0 < N; k0 += BK) {
-        for (int e = tid; e < BM * BK; e += 256) {
-            const int mm = e / BK, kk = e % BK;
-            const int m = m0 + mm, k = k0 + kk;
-            As[kk][mm] = (m < rows && k < N) ? snap[(size_t)m * N + k] : T(0);
-        }
-        for (int e = tid; e < BK * BL; e += 256) {
-            const int kk = e / BL, ll = e % BL;
-            const int k = k0 + kk, l = l0 + ll;
-            Ps[kk][ll] = (k < N && l < Lq) ? P[(size_t)k * Lq + l] : cplx<T>{T(0), T(0)};
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < BK; kk++) {
-            T a[4];
-            cplx<T> p[2];
-#pragma unroll
-            for (int u = 0; u < 4; u++) a[u] = As[kk][tm * 4 + u];
-#pragma unroll
-            for (int v = 0; v < 2; v++) p[v] = Ps[kk][tl * 2 + v];
-#pragma unroll
-            for (int u = 0; u < 4; u++)
-#pragma unroll
-                for (int v = 0; v < 2; v++) {
-                    ar[u][v][0] = fma(a[u], p[v].x, ar[u][v][0]);
-                    ar[u][v][1] = fma(a[u], p[v].y, ar[u][v][1]);
-                }
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int u = 0; u < 4; u++) {
-        const int m = m0 + tm * 4 + u;
-        if (m >= rows) continue;
-        const int c = m % 3, slot = m / 3, t = rec_begin + slot;
-        const T w = T(win[t]);
-#pragma unroll
-        for (int v = 0; v < 2; v++) {
-            const int l = l0 + tl * 2 + v;
-            if (l < Lq)
-                series[series_off<T>(s, c, qoff + l, t, nqb, n_rec_total)] = {w * ar[u][v][0], w * ar[u][v][1]};
-        }
-    }
-}
 
 // ---------------------------------------------------------- time transform
 
@@ -504,23 +437,6 @@ static auto time_kernel(int fl)
     case FK_GEN: return time_fft_kernel<T, FK_GEN>;
     default: return time_fft_kernel<T, FK_R3 | FK_GEN>;
     }
-}
-
-cudaError_t launch_list_proj_simt(const void *snap, int precision, int W, int R, int nrec_chunk,
-                                  int N, int rec_begin, int n_rec_total, const void *P, int Lq,
-                                  const double *win, void *series, int nqb, int qoff, cudaStream_t st)
-{
-    const int rows = nrec_chunk * 3;
-    dim3 grid((rows + 63) / 64, (Lq + 31) / 32, W);
-    if (precision == 0)
-        list_proj_simt_kernel<double><<<grid, 256, 0, st>>>(
-            (const double *)snap, rows, N, R, rec_begin, n_rec_total, (const cplx<double> *)P, Lq,
-            win, (cplx<double> *)series, nqb, qoff);
-    else
-        list_proj_simt_kernel<float><<<grid, 256, 0, st>>>(
-            (const float *)snap, rows, N, R, rec_begin, n_rec_total, (const cplx<float> *)P, Lq,
-            win, (cplx<float> *)series, nqb, qoff);
-    return cudaGetLastError();
 }
 
 int series_qblock(int precision) { return precision == 0 ? series_qb<double>() : series_qb<float>(); }

@@ -17,9 +17,7 @@
 // SMs the RK kernel leaves free.  After the last chunk the time-FFT kernel
 // transforms and squares every series and adds the sum over the wave's
 // samples into the job's accumulator.
-#include "../../include/smd_b200.h"
-#include "rk_cluster.cuh"
-#include "smd_launch.h"
+#include "host_internal.h"
 
 #include <cuda_runtime.h>
 
@@ -38,118 +36,15 @@
 #include <vector>
 
 using namespace smd;
+using namespace smdh;
 
 namespace {
 
-const char *kVersion = "smd_b200 0.1 (sm_100a)";
-
-struct DevBuf {
-    void *p = nullptr;
-    size_t bytes = 0;
-    ~DevBuf() { release(); }
-    void release()
-    {
-        if (p) cudaFree(p);
-        p = nullptr;
-        bytes = 0;
-    }
-    cudaError_t ensure(size_t b)
-    {
-        if (b <= bytes) return cudaSuccess;
-        release();
-        // below 1 GB, a quarter of headroom: a stream of growing jobs then
-        // reallocates (and synchronises the device) rarely
-        if (b < ((size_t)1 << 30)) b = (b + b / 4 + ((size_t)2 << 20) - 1) & ~(((size_t)2 << 20) - 1);
-        cudaError_t e = cudaMalloc(&p, b);
-        if (e == cudaSuccess) bytes = b;
-        else p = nullptr;
-        return e;
-    }
-    template <typename T>
-    T *as() const { return static_cast<T *>(p); }
-};
-
-// Partition of one lattice over a cluster of CS CTAs (see rk_cluster.cuh).
-struct ClusterTab {
-    ClusterParams P{};
-    DevBuf own_base, own_cnt, halo_cnt, halo_gid, idx, push;
-};
-
-struct Lattice {
-    int N = 0, G = 0, zn[3] = {0, 0, 0}, zoff[3] = {0, 0, 0}, ztot = 0;
-    bool lieb_delta = false;
-    bool vac_only = true;           // impurities (if any) have zero couplings
-    LatticeDev dev{};
-    DevBuf nbr, grid_map, bonds;
-    std::vector<double> pos;
-    std::vector<int> nbr_h[3];      // host copies of the active shells' tables
-    std::map<int, std::unique_ptr<ClusterTab>> ctabs;   // keyed by CTAs per sample
-    std::mutex cache_mu;            // guards ctabs
-};
-
-struct QSet {
-    int lattice = -1;
-    int use_grid = 0;
-    int G = 0;
-    int n_list = 0;
-    int Q = 0;
-    double list_scale = 1.0;
-    int fp64_ok = 1;           // the FP64 grid transform fits (one block or two passes)
-    int large[2] = {0, 0};     // per precision (0 FP64, 1 FP32): two-pass transform
-    FFTPlan gplan{};
-    DevBuf tw64, tw32;        // grid twiddles
-    DevBuf phase64, phase32;  // [N][n_list] complex
-    // tensor-core operand of the FP32 form: rows 2l / 2l + 1 hold
-    // scale cos(q_l . r_k) / -scale sin(q_l . r_k), split into bf16 high and
-    // low parts, row pitch kp
-    int kp = 0;
-    DevBuf bhi, blo;
-    CUtensorMap map_bhi{}, map_blo{};
-};
-
-struct Plan {
-    FFTPlan p{};
-    DevBuf tw64, tw32;
-};
+const char *kVersion = "smd_b200 0.2 (sm_100a)";
 
 }  // namespace
 
-// Snapshot buffers between the integration and projection streams: the RK
-// launch of chunk c reuses the buffer of chunk c - kSnapBufs, so the
-// projection has kSnapBufs - 1 RK launches' time to catch up before the
-// integration waits for it.
-constexpr int kSnapBufs = 3;
-
-struct smd_ctx {
-    int device = 0;
-    size_t budget = 0;
-    cudaStream_t s_rk = nullptr, s_proj = nullptr;
-    cudaEvent_t ev_rk[kSnapBufs]{}, ev_proj[kSnapBufs]{};
-    cudaEvent_t ev_tf[3]{};   // per-component time transforms done (host copy may start)
-    cudaEvent_t t0 = nullptr, t1 = nullptr;
-    std::string err;
-    int next_id = 1;
-    // lattices and q sets are shared with the serving lanes' contexts
-    // (smd_share_objects); maps_mu guards the maps
-    std::mutex maps_mu;
-    std::map<int, std::shared_ptr<Lattice>> lattices;
-    std::map<int, std::shared_ptr<QSet>> qsets;
-    std::map<int, std::unique_ptr<Plan>> tplans;   // keyed by n
-    // job buffers (grow-only)
-    DevBuf state, s0, imp, snap[kSnapBufs], series, qss, stats, e0, status, win, acc_tmp, in_tmp, out_tmp;
-    DevBuf gscratch;   // packed row-transformed grids of the two-pass grid transform
-    DevBuf qpart;      // cluster kernel: per-CTA autocorrelation partials [W][n_rec][CS]
-    int launches = 0;
-    std::vector<cudaEvent_t> tev;   // timing events, reused across calls
-    // split-BF16 snapshot rows and their tensor maps, one pair per snapshot
-    // buffer
-    DevBuf ahi[kSnapBufs], alo[kSnapBufs];
-    CUtensorMap map_ahi[kSnapBufs]{}, map_alo[kSnapBufs]{};
-    const void *map_a_base[kSnapBufs]{};
-    int map_a_rows[kSnapBufs]{}, map_a_kp[kSnapBufs]{};
-};
-
-namespace {
+namespace smdh {
 
 int fail(smd_ctx *c, int code, const std::string &msg)
 {
@@ -161,12 +56,6 @@ int cuda_fail(smd_ctx *c, cudaError_t e, const char *where)
 {
     return fail(c, SMD_ECUDA, std::string(where) + ": " + cudaGetErrorString(e));
 }
-
-#define CK(expr, where)                                   \
-    do {                                                  \
-        cudaError_t _e = (expr);                          \
-        if (_e != cudaSuccess) return cuda_fail(ctx, _e, where); \
-    } while (0)
 
 // Radices of an FFT of length n.  wide: radix 16 and 8 first (the grid
 // transform, whose stages hold 16 values per thread), else radix 4 first.
@@ -237,6 +126,10 @@ cudaError_t upload_twiddles(int n, DevBuf &d64, DevBuf &d32)
     if (e != cudaSuccess) return e;
     return cudaMemcpy(d32.p, wf.data(), wf.size() * sizeof(float), cudaMemcpyHostToDevice);
 }
+
+}  // namespace smdh
+
+namespace {
 
 // E = 1/2 sum_i (S_i . h_i - h S_i^z) equals the bond sum when every
 // neighbour relation is a bond listed once, present in both directions in
@@ -334,6 +227,7 @@ extern "C" int smd_ctx_destroy(smd_ctx *ctx)
     if (!ctx) return SMD_EINVAL;
     cudaSetDevice(ctx->device);
     cudaDeviceSynchronize();
+    ctx->batches.clear();
     ctx->lattices.clear();
     ctx->qsets.clear();
     ctx->tplans.clear();
@@ -517,11 +411,8 @@ extern "C" int smd_qset_upload(smd_ctx *ctx, int lattice_id, int use_grid, int n
                 ph[2 * ((size_t)k * n_list + l)] = list_scale * std::cos(a);
                 ph[2 * ((size_t)k * n_list + l) + 1] = list_scale * std::sin(a);
             }
-        std::vector<float> pf(ph.begin(), ph.end());
         CK(Q->phase64.ensure(ph.size() * sizeof(double)), "cudaMalloc");
         CK(cudaMemcpy(Q->phase64.p, ph.data(), ph.size() * sizeof(double), cudaMemcpyHostToDevice), "H2D");
-        CK(Q->phase32.ensure(pf.size() * sizeof(float)), "cudaMalloc");
-        CK(cudaMemcpy(Q->phase32.p, pf.data(), pf.size() * sizeof(float), cudaMemcpyHostToDevice), "H2D");
         // split-bf16 operand of the tensor-core projection, [2 n_list][kp]
         const int kp = tc_kpitch(N);
         Q->kp = kp;
@@ -562,31 +453,55 @@ extern "C" int smd_qset_size(smd_ctx *ctx, int qset_id, int *Q)
     return SMD_OK;
 }
 
-namespace {
+namespace smdh {
 
-struct JobGeom {
-    Lattice *L;
-    QSet *Qs;
-    Plan *tp;
-    int N, Q, nqb, n_rec, prec, R, W, waves;   // nqb: q blocks of the series layout
-    size_t elem, celem;
-    ClusterTab *ctab = nullptr;   // cluster kernel partition (null: single-CTA kernel)
-    int spt = 0, threads = 0;
-};
+std::shared_ptr<Lattice> find_lattice(smd_ctx *ctx, int id)
+{
+    std::lock_guard<std::mutex> lk(ctx->maps_mu);
+    auto it = ctx->lattices.find(id);
+    return it == ctx->lattices.end() ? nullptr : it->second;
+}
+
+std::shared_ptr<QSet> find_qset(smd_ctx *ctx, int id)
+{
+    std::lock_guard<std::mutex> lk(ctx->maps_mu);
+    auto it = ctx->qsets.find(id);
+    return it == ctx->qsets.end() ? nullptr : it->second;
+}
+
+int time_plan(smd_ctx *ctx, int n, Plan **out)
+{
+    auto pi = ctx->tplans.find(n);
+    if (pi == ctx->tplans.end()) {
+        auto P = std::make_unique<Plan>();
+        if (!make_plan(n, P->p, false)) return fail(ctx, SMD_EINVAL, "job: n_rec has a prime factor > 64");
+        CK(upload_twiddles(n, P->tw64, P->tw32), "twiddles");
+        pi = ctx->tplans.emplace(n, std::move(P)).first;
+    }
+    *out = pi->second.get();
+    return SMD_OK;
+}
+
+bool cluster_ok(const Lattice &L)
+{
+    return L.dev.energy_from_field && !L.lieb_delta && L.vac_only;
+}
 
 // Partition of lattice L over CS CTAs: contiguous site ranges, halo lists,
-// packed local neighbour slots and halo push lists.  Null when the lattice
-// does not fit the cluster kernel's limits.
-ClusterTab *cluster_tables(Lattice &L, int CS)
+// packed local neighbour slots and halo push lists.  Edge slots beyond the
+// lattice's neighbours (up to the kernel's ZT) name the zero pad slot.
+// Null when the lattice does not fit the cluster kernel's limits.
+ClusterTab *cluster_tables(Lattice &L, int CS, int zt_min)
 {
-    std::lock_guard<std::mutex> lk(L.cache_mu);
-    auto it = L.ctabs.find(CS);
-    if (it != L.ctabs.end()) return it->second.get();
     const int N = L.N;
     if (CS < 1 || CS > kMaxClusterCTAs || N < CS) return nullptr;
     const int zact = L.zn[0] + L.zn[1] + L.zn[2];
-    const int ZT = zact <= 4 ? 4 : zact <= 8 ? 8 : zact <= 12 ? 12 : zact <= 18 ? 18 : -1;
+    const int zneed = std::max(zact, zt_min);
+    const int ZT = zneed <= 4 ? 4 : zneed <= 8 ? 8 : zneed <= 12 ? 12 : zneed <= 18 ? 18 : -1;
     if (ZT < 0) return nullptr;
+    std::lock_guard<std::mutex> lk(L.cache_mu);
+    auto it = L.ctabs.find({CS, ZT});
+    if (it != L.ctabs.end()) return it->second.get();
     std::vector<int> base(CS + 1), owner(N);
     for (int r = 0; r <= CS; r++) base[r] = (int)((long long)N * r / CS);
     for (int r = 0; r < CS; r++)
@@ -722,9 +637,67 @@ ClusterTab *cluster_tables(Lattice &L, int CS)
     P.idx = T->idx.as<uint32_t>();
     P.push = T->push.as<int>();
     ClusterTab *raw = T.get();
-    L.ctabs[CS] = std::move(T);
+    L.ctabs[{CS, ZT}] = std::move(T);
     return raw;
 }
+
+int project_chunk(smd_ctx *ctx, const ProjArgs &a, cudaStream_t st, int *launches)
+{
+    Lattice &L = *a.L;
+    QSet &Qs = *a.Qs;
+    const int n = a.re - a.rb;
+    const int p32 = a.prec == SMD_FP64 ? 0 : 1;
+    if (Qs.use_grid) {
+        const double scale = std::sqrt(1.0 / ((double)Qs.G * Qs.G));   // subrouts.cpp:8343
+        const void *tw = p32 ? Qs.tw32.p : Qs.tw64.p;
+        if (Qs.large[p32]) {
+            CK(a.gscratch->ensure((size_t)a.W * grid_large_scratch(Qs.G, a.R, p32)), "cudaMalloc grid scratch");
+            CK(launch_grid_proj_large(a.snap, a.prec, a.N, a.W, a.R, n, a.rb, a.n_rec, L.grid_map.as<int>(),
+                                      Qs.gplan, tw, scale, a.win, a.series, a.nqb, a.gscratch->p, st),
+               "grid projection (two passes)");
+            *launches += 2;
+        } else {
+            CK(launch_grid_proj(a.snap, a.prec, a.N, a.W, a.R, n, a.rb, a.n_rec, L.grid_map.as<int>(), Qs.gplan,
+                                tw, scale, a.win, a.series, a.nqb, st),
+               "grid projection");
+            *launches += 1;
+        }
+    }
+    if (Qs.n_list > 0 && p32) {
+        // split-BF16 tensor-core projection of the chunk's rows
+        const int rows = a.W * a.R * 3;
+        if (!a.fused_split) {
+            CK(launch_split_bf16(static_cast<const float *>(a.snap), rows, a.N, Qs.kp, a.ahi, a.alo, st),
+               "bf16 split");
+            *launches += 1;
+        }
+        CK(launch_list_proj_tc(*a.map_ahi, *a.map_alo, Qs.map_bhi, Qs.map_blo, rows, Qs.kp, a.R, n, a.rb,
+                               a.n_rec, Qs.n_list, a.win, a.series, a.nqb, Qs.G * Qs.G, a.status, st),
+           "tensor-core list projection");
+        *launches += 1;
+    } else if (Qs.n_list > 0) {
+        CK(launch_list_proj_f64(static_cast<const double *>(a.snap), a.W, a.R, n, a.N, a.rb, a.n_rec,
+                                Qs.phase64.as<double>(), Qs.n_list, a.win, a.series, a.nqb, Qs.G * Qs.G, st),
+           "FP64 list projection");
+        *launches += 1;
+    }
+    return SMD_OK;
+}
+
+}  // namespace smdh
+
+namespace {
+
+struct JobGeom {
+    Lattice *L;
+    QSet *Qs;
+    Plan *tp;
+    int N, Q, nqb, n_rec, prec, R, W, waves;   // nqb: q blocks of the series layout
+    size_t elem, celem;
+    ClusterTab *ctab = nullptr;   // cluster kernel partition (null: single-CTA kernel)
+    int spt = 0, threads = 0;
+};
+
 
 // Cluster size and thread shape for a job.  Lattices the cluster kernel does
 // not cover (bond-list energies, the Lieb d-wave term, impurities with
@@ -735,7 +708,7 @@ void choose_cluster(smd_ctx *ctx, JobGeom &g, int n_samples)
 {
     Lattice &L = *g.L;
     g.ctab = nullptr;
-    if (!L.dev.energy_from_field || L.lieb_delta || !L.vac_only) return;
+    if (!cluster_ok(L)) return;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
     int forced = 0;
@@ -797,14 +770,10 @@ int prepare(smd_ctx *ctx, const smd_job_desc *job, JobGeom &g)
         return fail(ctx, SMD_EINVAL, "job: grid too large for the FP64 shared-memory transform");
     g.elem = g.prec == SMD_FP64 ? sizeof(double) : sizeof(float);
     g.celem = 2 * g.elem;
-    auto pi = ctx->tplans.find(g.n_rec);
-    if (pi == ctx->tplans.end()) {
-        auto P = std::make_unique<Plan>();
-        if (!make_plan(g.n_rec, P->p, false)) return fail(ctx, SMD_EINVAL, "job: n_rec has a prime factor > 64");
-        CK(upload_twiddles(g.n_rec, P->tw64, P->tw32), "twiddles");
-        pi = ctx->tplans.emplace(g.n_rec, std::move(P)).first;
+    {
+        int rc = time_plan(ctx, g.n_rec, &g.tp);
+        if (rc) return rc;
     }
-    g.tp = pi->second.get();
     if (!time_fft_fits(g.n_rec, g.prec, g.tp->p))
         return fail(ctx, SMD_EINVAL, "job: n_rec too long for the shared-memory time transform");
     // chunk of records per RK launch (C2 measured: 128 records 129.4 ms per
@@ -952,44 +921,30 @@ int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const do
             CK(cudaEventRecord(ctx->ev_rk[b], ctx->s_rk), "event");
             CK(cudaStreamWaitEvent(ctx->s_proj, ctx->ev_rk[b], 0), "wait");
             CK(cudaEventRecord(ev(2 + 2 * nchunks + 2 * c), ctx->s_proj), "event");
-            if (Qs.use_grid) {
-                const double scale = std::sqrt(1.0 / ((double)Qs.G * Qs.G));   // subrouts.cpp:8343
-                if (Qs.large[g.prec == SMD_FP64 ? 0 : 1]) {
-                    CK(ctx->gscratch.ensure((size_t)W * grid_large_scratch(Qs.G, R, g.prec == SMD_FP64 ? 0 : 1)),
-                       "cudaMalloc grid scratch");
-                    CK(launch_grid_proj_large(ctx->snap[b].p, g.prec, N, Ww, R, re - rb, rb, n_rec,
-                                              L.grid_map.as<int>(), Qs.gplan,
-                                              g.prec == SMD_FP64 ? Qs.tw64.p : Qs.tw32.p, scale, d_win,
-                                              ctx->series.p, nqb, ctx->gscratch.p, ctx->s_proj),
-                       "grid projection (two passes)");
-                    ctx->launches += 2;
-                } else {
-                    CK(launch_grid_proj(ctx->snap[b].p, g.prec, N, Ww, R, re - rb, rb, n_rec,
-                                        L.grid_map.as<int>(), Qs.gplan,
-                                        g.prec == SMD_FP64 ? Qs.tw64.p : Qs.tw32.p, scale, d_win,
-                                        ctx->series.p, nqb, ctx->s_proj), "grid projection");
-                    ctx->launches++;
-                }
-            }
-            if (tc_list) {
-                // split-BF16 tensor-core projection of the chunk's rows
-                const int rows = Ww * R * 3, kp = Qs.kp;
-                if (!fused_split) {
-                    CK(launch_split_bf16(ctx->snap[b].as<float>(), rows, N, kp, ctx->ahi[b].p,
-                                         ctx->alo[b].p, ctx->s_proj), "bf16 split");
-                    ctx->launches++;
-                }
-                CK(launch_list_proj_tc(ctx->map_ahi[b], ctx->map_alo[b], Qs.map_bhi, Qs.map_blo, rows,
-                                       kp, R, re - rb, rb, n_rec, Qs.n_list, d_win, ctx->series.p, nqb,
-                                       Qs.G * Qs.G, ctx->status.as<int>(), ctx->s_proj),
-                   "tensor-core list projection");
-                ctx->launches++;
-            } else if (Qs.n_list > 0) {
-                CK(launch_list_proj_simt(ctx->snap[b].p, g.prec, Ww, R, re - rb, N, rb, n_rec,
-                                         Qs.phase64.p, Qs.n_list, d_win, ctx->series.p, nqb, Qs.G * Qs.G,
-                                         ctx->s_proj),
-                   "list projection");
-                ctx->launches++;
+            ProjArgs pa{};
+            pa.L = &L;
+            pa.Qs = &Qs;
+            pa.prec = g.prec;
+            pa.N = N;
+            pa.W = Ww;
+            pa.R = R;
+            pa.rb = rb;
+            pa.re = re;
+            pa.n_rec = n_rec;
+            pa.nqb = nqb;
+            pa.snap = ctx->snap[b].p;
+            pa.ahi = ctx->ahi[b].p;
+            pa.alo = ctx->alo[b].p;
+            pa.map_ahi = &ctx->map_ahi[b];
+            pa.map_alo = &ctx->map_alo[b];
+            pa.fused_split = fused_split;
+            pa.win = d_win;
+            pa.series = ctx->series.p;
+            pa.gscratch = &ctx->gscratch;
+            pa.status = ctx->status.as<int>();
+            {
+                int rc = project_chunk(ctx, pa, ctx->s_proj, &ctx->launches);
+                if (rc) return rc;
             }
             CK(cudaEventRecord(ev(3 + 2 * nchunks + 2 * c), ctx->s_proj), "event");
             CK(cudaEventRecord(ctx->ev_proj[b], ctx->s_proj), "event");

@@ -48,6 +48,36 @@ struct ClusterParams {
     const int *push;       // [CS][pmax][n_own_max] (rank << 16 | slot) or -1
 };
 
+// Batched form: one persistent launch integrates the samples of several
+// lattices (slots), each with its own partition, coefficients and buffers.
+// Clusters of CSH CTAs take work items (slot, first sample) from a device
+// queue; a slot whose partition has CS <= CSH CTAs (CS dividing CSH) runs
+// CSH / CS samples per item, one per group of CS CTAs.  The item list is
+// ordered by the host (largest per-CTA work first).
+constexpr int kMaxBatchSlots = 24;
+
+struct BatchSlot {
+    ClusterParams P;   // partition of the slot's lattice (P.CS CTAs per sample)
+    RKJob J;           // the slot's buffers and record range for this launch
+};
+
+struct BatchParams {
+    int n_slots;
+    int n_items;
+    const int2 *items;   // [n_items]: (slot, first sample of the item)
+    int *queue;          // next item; zero before the launch
+    BatchSlot slot[kMaxBatchSlots];
+};
+
+// Launch of the persistent batch kernel: nclusters clusters of csh CTAs of
+// `threads` threads each; zt = edge slots of every slot's tables.
+cudaError_t launch_rk_batch(const BatchParams &B, int precision, int spt, int zt, int threads, int csh,
+                            int nclusters, size_t smem, cudaStream_t st);
+// Clusters of the batch kernel that fit the device at once (0 if none).
+int rk_batch_max_clusters(int precision, int spt, int zt, int threads, int csh, size_t smem);
+// Threads per CTA of the batch kernel for a sites-per-thread value.
+int rk_batch_threads(int precision, int spt);
+
 size_t rk_cluster_smem(const ClusterParams &P, int precision);
 // qss[s][r] = r == 0 ? 1 : (1 / N) * sum over the CS partials of record r,
 // summed in rank order (the order of the in-cluster reduction)

@@ -87,16 +87,20 @@ __host__ __device__ constexpr int cl_maxt(int spt)
     return spt <= 1 ? 768 : spt <= 2 ? 576 : 512;
 }
 
+// One RK launch's records for one sample, spread over the CS CTAs of a group
+// of the thread-block cluster: this CTA is CTA `rank` of the group, whose
+// CTA 0 is the cluster's CTA `vbase` (every distributed-shared-memory access
+// and halo push addresses vbase + the group rank).  All CTAs of the
+// hardware cluster run this function together on samples of the same
+// lattice and record range, so they meet the same cluster barriers.
 template <typename T, int SPT, int ZT>
-__global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
-    rk_cluster_kernel(const ClusterParams P, const RKJob J)
+__device__ __forceinline__ void rk_sample(const ClusterParams &P, const RKJob &J, const int smp,
+                                          const int rank, const int vbase,
+                                          unsigned char *smem_raw)
 {
     static_assert(ZT % 2 == 0 && ZT <= kMaxEdgeSlots, "edge slots come in packed pairs");
-    extern __shared__ __align__(32) unsigned char smem_raw[];
     cg::cluster_group cl = cg::this_cluster();
     const int CS = P.CS;
-    const int rank = (int)cl.block_rank();
-    const int smp = blockIdx.x / CS;
     const int NT = blockDim.x, tid = threadIdx.x;
     const int N = P.N;
     const int base = P.own_base[rank], n_own = P.own_cnt[rank], n_halo = P.halo_cnt[rank];
@@ -253,7 +257,7 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
                 x = warp_sum_c(x);
                 if (lane == 0) {
                     for (int r = 0; r < CS; r++) {
-                        double *rr = cl.map_shared_rank(red, r) + ((slot * kMaxClusterCTAs + rank) * 4 + q) * 2;
+                        double *rr = cl.map_shared_rank(red, vbase + r) + ((slot * kMaxClusterCTAs + rank) * 4 + q) * 2;
                         rr[0] = x.s;
                         rr[1] = x.c;
                     }
@@ -278,8 +282,8 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
         if (AH) {
             const uint32_t la = (uint32_t)__cvta_generic_to_shared(buf + (code & 0xffff));
             uint32_t ra, rb;
-            asm("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(ra) : "r"(la), "r"(code >> 16));
-            asm("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(rb) : "r"(cur_bar), "r"(code >> 16));
+            asm("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(ra) : "r"(la), "r"(vbase + (code >> 16)));
+            asm("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(rb) : "r"(cur_bar), "r"(vbase + (code >> 16)));
             if constexpr (sizeof(T) == 4) {
                 asm volatile(
                     "st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.f32 [%0], {%1, %2, %3, %4}, [%5];" ::"r"(ra),
@@ -294,7 +298,7 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
                              : "memory");
             }
         } else {
-            cl.map_shared_rank(buf, code >> 16)[code & 0xffff] = v;
+            cl.map_shared_rank(buf, vbase + (code >> 16))[code & 0xffff] = v;
         }
     };
     auto put = [&](Vec4<T> *buf, int k, int li, const Vec4<T> &v) {
@@ -315,7 +319,7 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
         for (int p = 0; p < P.pmax; p++) {
             const int code = push[p * nom + li];
             if (code >= 0) {
-                double *rd = cl.map_shared_rank(D, code >> 16);
+                double *rd = cl.map_shared_rank(D, vbase + (code >> 16));
                 const int s2 = code & 0xffff;
                 for (int c = 0; c < 3; c++) rd[c * Np + s2] = v[c];
             }
@@ -748,6 +752,105 @@ __global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
     }
     if (rank == 0 && tid == 0) J.stats[smp * 4 + 0] = drift;
     cl_sync();   // no CTA leaves while others may still touch its shared memory
+    if (AH && tid == 0) {
+        // every publish to this CTA has completed (the last one was awaited
+        // above): the barriers can be set up afresh for the next sample
+        asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(hbar_a) : "memory");
+        asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(hbar_a + 8u) : "memory");
+    }
+}
+
+// One sample per cluster of P.CS CTAs: sample blockIdx.x / P.CS.
+template <typename T, int SPT, int ZT>
+__global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
+    rk_cluster_kernel(const ClusterParams P, const RKJob J)
+{
+    extern __shared__ __align__(32) unsigned char smem_raw[];
+    const int rank = (int)cg::this_cluster().block_rank();
+    rk_sample<T, SPT, ZT>(P, J, blockIdx.x / P.CS, rank, 0, smem_raw);
+}
+
+// Persistent batch kernel: clusters take items from B.queue until it runs
+// dry.  The slot loop runs over a uniform index so that the slot's
+// parameters are read from the kernel-parameter bank at a uniform address
+// (the coefficients stay constant operands); only the matching slot runs.
+template <typename T, int SPT, int ZT>
+__global__ void __launch_bounds__(cl_maxt<T>(SPT), 1)
+    rk_batch_kernel(const __grid_constant__ BatchParams B)
+{
+    extern __shared__ __align__(32) unsigned char smem_raw[];
+    __shared__ int item_s;
+    cg::cluster_group cl = cg::this_cluster();
+    const int hw = (int)cl.block_rank(), csh = (int)cl.num_blocks();
+    for (;;) {
+        if (hw == 0 && threadIdx.x == 0) {
+            const int it = atomicAdd(B.queue, 1);
+            for (int r = 0; r < csh; r++) *cl.map_shared_rank(&item_s, r) = it;
+        }
+        cl.sync();
+        const int it = item_s;
+        if (it >= B.n_items) break;
+        const int2 w = B.items[it];
+        for (int lu = 0; lu < B.n_slots; lu++) {
+            if (lu != w.x) continue;
+            const int vcs = B.slot[lu].P.CS, g = hw / vcs;
+            rk_sample<T, SPT, ZT>(B.slot[lu].P, B.slot[lu].J, w.y + g, hw - g * vcs, g * vcs, smem_raw);
+        }
+        cl.sync();   // every CTA has read item_s before rank 0 overwrites it
+    }
+}
+
+template <typename T, int SPT, int ZT>
+cudaError_t launch_batch_t(const BatchParams *B, int threads, int csh, int nclusters, size_t smem,
+                           cudaStream_t st, int *max_clusters)
+{
+    auto k = rk_batch_kernel<T, SPT, ZT>;
+    cudaError_t e = allow_dynamic_smem(k);
+    if (e != cudaSuccess) return e;
+    if (csh > 8) {
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e != cudaSuccess) return e;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(nclusters * csh), 1, 1);
+    cfg.blockDim = dim3(threads, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = csh;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (max_clusters) {
+        cfg.gridDim = dim3((unsigned)csh, 1, 1);
+        return cudaOccupancyMaxActiveClusters(max_clusters, k, &cfg);
+    }
+    return cudaLaunchKernelEx(&cfg, k, *B);
+}
+
+template <typename T, int SPT>
+cudaError_t launch_batch_spt(const BatchParams *B, int zt, int threads, int csh, int nclusters, size_t smem,
+                             cudaStream_t st, int *max_clusters)
+{
+    switch (zt) {
+    case 8: return launch_batch_t<T, SPT, 8>(B, threads, csh, nclusters, smem, st, max_clusters);
+    case 12: return launch_batch_t<T, SPT, 12>(B, threads, csh, nclusters, smem, st, max_clusters);
+    case 18: return launch_batch_t<T, SPT, 18>(B, threads, csh, nclusters, smem, st, max_clusters);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+template <typename T>
+cudaError_t launch_batch_prec(const BatchParams *B, int spt, int zt, int threads, int csh, int nclusters,
+                              size_t smem, cudaStream_t st, int *max_clusters)
+{
+    switch (spt) {
+    case 2: return launch_batch_spt<T, 2>(B, zt, threads, csh, nclusters, smem, st, max_clusters);
+    case 4: return launch_batch_spt<T, 4>(B, zt, threads, csh, nclusters, smem, st, max_clusters);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 template <typename T, int SPT, int ZT>

@@ -29,9 +29,10 @@ cudaError_t launch_grid_proj(const void *snap, int precision, int N, int W, int 
                              int rec_begin, int n_rec_total, const int *grid_map,
                              const FFTPlan &plan, const void *tw, double scale, const double *win,
                              void *series, int nqb, cudaStream_t st);
-cudaError_t launch_list_proj_simt(const void *snap, int precision, int W, int R, int nrec_chunk,
-                                  int N, int rec_begin, int n_rec_total, const void *P, int Lq,
-                                  const double *win, void *series, int nqb, int qoff, cudaStream_t st);
+// FP64 list projection on the FP64 tensor cores (proj_f64.cu)
+cudaError_t launch_list_proj_f64(const double *snap, int W, int R, int nrec_chunk, int N, int rec_begin,
+                                 int n_rec_total, const double *P, int Lq, const double *win, void *series,
+                                 int nqb, int qoff, cudaStream_t st);
 // q values per block of the series layout (series_qb) of a precision
 int series_qblock(int precision);
 int time_fft_qt(int n, int precision);

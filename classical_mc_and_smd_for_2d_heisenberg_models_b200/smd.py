@@ -290,6 +290,13 @@ class Context:
             spinField[...] = sf
         return x, y, z, q
 
+    # -- batches
+    def batch(self, members, dt: float, n_rec: int, stride: int = 1, precision: int = SMD_FP32,
+              fix_every: int = 16) -> "Batch":
+        """A batched job over several lattices.  members: [(lattice_id,
+        qset_id, n_samples, imp or None)]."""
+        return Batch(self, members, dt, n_rec, stride, precision, fix_every)
+
     # -- serving
     def submit(self, lattice_id, qset_id, spins, dt, n_rec, stride=1, precision=SMD_FP64,
                fix_every=1, win=None, imp=None):
@@ -322,3 +329,62 @@ class Context:
 
     def cancel(self, job_id: int) -> int:
         return self.lib.smd_cancel(self.h, job_id)
+
+
+class Batch:
+    """Several jobs on different lattices run as one batch (smd_batch_*):
+    one persistent RK launch per chunk of records for every member, the job
+    step replayed as one CUDA graph.  ``run`` returns each member's sample
+    averages as a RunResult (final spins are not kept)."""
+
+    def __init__(self, ctx: Context, members, dt, n_rec, stride, precision, fix_every):
+        self.ctx = ctx
+        self.n_rec = n_rec
+        self._imps = []
+        arr = (_lib.BatchMember * len(members))()
+        self.sizes = []
+        for k, (lid, qid, ns, imp) in enumerate(members):
+            arr[k].lattice, arr[k].qset, arr[k].n_samples = lid, qid, ns
+            if imp is not None:
+                ia = np.ascontiguousarray(imp, np.int32)
+                self._imps.append(ia)
+                arr[k].imp = ia.ctypes.data
+            lat, _ = ctx._keep[("lat", lid)]
+            self.sizes.append((ns, lat.N, ctx.qset_size(qid)))
+        d = _lib.BatchDesc()
+        d.n_members = len(members)
+        d.members = arr
+        d.dt, d.n_rec, d.stride, d.precision, d.fix_every = dt, n_rec, stride, precision, fix_every
+        bid = C.c_int()
+        ctx._check(ctx.lib.smd_batch_create(ctx.h, C.byref(d), C.byref(bid)), "smd_batch_create")
+        self.id = bid.value
+
+    def info(self) -> dict:
+        t = _lib.BatchTuning()
+        self.ctx._check(self.ctx.lib.smd_batch_info(self.ctx.h, self.id, C.byref(t)), "smd_batch_info")
+        out = {k: getattr(t, k) for k, _ in _lib.BatchTuning._fields_ if k != "member_ctas"}
+        out["member_ctas"] = [t.member_ctas[i] for i in range(len(self.sizes))]
+        return out
+
+    def run(self, spins, win=None):
+        """spins: one [S][N][3] array per member; returns [RunResult]."""
+        n = self.n_rec
+        win = np.ones(n) if win is None else np.ascontiguousarray(win, np.float64)
+        sp = [np.ascontiguousarray(x, np.float64) for x in spins]
+        spec = [np.zeros((3, Q, n)) for (_, _, Q) in self.sizes]
+        qss = [np.zeros(n) for _ in self.sizes]
+        k = len(sp)
+        P = C.POINTER(C.c_double)
+        ins = (P * k)(*[_dp(x) for x in sp])
+        so = (P * k)(*[_dp(x) for x in spec])
+        qo = (P * k)(*[_dp(x) for x in qss])
+        rep = _lib.Report()
+        self.ctx._check(self.ctx.lib.smd_batch_run(self.ctx.h, self.id, ins, _dp(win), so, qo,
+                                                   C.byref(rep)), "smd_batch_run")
+        report = {f: getattr(rep, f) for f, _ in _lib.Report._fields_}
+        return [RunResult(spec[i], qss[i], None, report) for i in range(k)]
+
+    def free(self):
+        if self.id is not None:
+            self.ctx.lib.smd_batch_free(self.ctx.h, self.id)
+            self.id = None

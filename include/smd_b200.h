@@ -165,7 +165,7 @@ typedef struct {
     double ms_proj;        /* summed duration of the projection launches */
     double ms_tfft;        /* summed duration of the time-transform launches */
     int rk_launches;       /* RK kernel launches */
-    int rk_kind;           /* RK kernel used: 0 single-CTA, 1 cluster */
+    int rk_kind;           /* RK kernel used: 0 single-CTA, 1 cluster, 3 batch (smd_batch_run) */
     int rk_ctas;           /* CTAs per sample (cluster size) */
 } smd_report;
 
@@ -203,6 +203,65 @@ SMD_API int smd_dyn_spectrum_ref(smd_ctx *ctx, int lattice_id, int qset_id, doub
 SMD_API int smd_evolve(smd_ctx *ctx, int lattice_id, int precision, int n_samples,
                double dt, int nsteps, int fix_every, const int *imp,
                double *spins, smd_report *rep);
+
+/* ------------------------------------------------------------- batches */
+
+/* Batched form: the sample loops of several jobs on different lattices
+ * (the reference runs one lattice per xSMD_run, one sample at a time in
+ * Codes_Folder/smd_code.cpp:3079-3311) integrated by one persistent RK
+ * launch per chunk of records.  Thread-block clusters take (lattice, sample)
+ * work items from a device queue, so lattices of uneven N share the SMs;
+ * the projections and time transforms follow per lattice, and the whole
+ * job step is replayed as one CUDA graph.  Members share dt, n_rec, stride,
+ * precision and correction period; each has its own q set and samples.
+ * Every member's lattice must suit the cluster kernel (energies from the
+ * field identity, no Lieb d-wave term, impurities only as vacancies).
+ * A project-written autotuner picks the cluster size, sites per thread and
+ * records per launch for the batch's shape on first use (cached per shape
+ * in the process; smd_batch_info reports the choice). */
+typedef struct {
+    int lattice;           /* lattice id */
+    int qset;              /* q set on that lattice */
+    int n_samples;         /* samples of this member */
+    const int *imp;        /* [n_samples][N] impurity flags, or NULL */
+} smd_batch_member;
+
+typedef struct {
+    int n_members;                    /* 1 .. 24 */
+    const smd_batch_member *members;
+    double dt;
+    int n_rec, stride, precision, fix_every;
+} smd_batch_desc;
+
+typedef struct {
+    int cluster_ctas;      /* CTAs per thread-block cluster of the RK launch */
+    int sites_per_thread;  /* largest own sites per thread */
+    int threads;           /* threads per CTA */
+    int edge_slots;        /* neighbour slots per site (padded) */
+    int records_per_launch;
+    int clusters;          /* persistent clusters of the RK launch */
+    int items;             /* work items per RK launch */
+    int candidates;        /* configurations timed by the autotuner (0: cached) */
+    double probe_ms;       /* autotuner time spent */
+    int member_ctas[24];   /* CTAs per sample of each member */
+} smd_batch_tuning;
+
+/* Plan, tune and allocate a batch (device buffers for every member: HBM
+ * footprint beyond the context's budget gives SMD_ENOMEM_ADMIT). */
+SMD_API int smd_batch_create(smd_ctx *ctx, const smd_batch_desc *desc, int *batch_id);
+SMD_API int smd_batch_info(smd_ctx *ctx, int batch_id, smd_batch_tuning *out);
+/* One job step of every member from host buffers: spins0[m] is
+ * [n_samples][N][3] (host), window [n_rec]; spec_out[m] [3][Q_m][n_rec] and
+ * qss_out[m] [n_rec] receive the member's sample averages (as smd_run). */
+SMD_API int smd_batch_run(smd_ctx *ctx, int batch_id, const double *const *spins0,
+                          const double *window, double *const *spec_out,
+                          double *const *qss_out, smd_report *rep);
+/* The same from device buffers; d_spec_sum[m] / d_qss_sum[m] receive the
+ * member's sample SUMS (written, not accumulated). */
+SMD_API int smd_batch_run_device(smd_ctx *ctx, int batch_id, const double *const *d_spins0,
+                                 const double *d_window, double *const *d_spec_sum,
+                                 double *const *d_qss_sum, smd_report *rep);
+SMD_API int smd_batch_free(smd_ctx *ctx, int batch_id);
 
 /* ------------------------------------------------------------- serving */
 
