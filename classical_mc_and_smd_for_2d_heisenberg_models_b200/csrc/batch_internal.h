@@ -49,6 +49,18 @@ int member_finish(smd_ctx *ctx, Member &mb, double *acc, double *accq, cudaStrea
 // padded samples repeat the last sample.
 int member_load(smd_ctx *ctx, Member &mb, const double *d_spins, cudaStream_t st, int *launches);
 
+// Work items (slot, first sample) of one launch over members with CTAs per
+// sample vcs[i] in clusters of csh CTAs (csh / vcs[i] samples per item),
+// the costliest members first.
+std::vector<int2> make_items(const std::vector<Member *> &m, const std::vector<int> &vcs, int csh);
+// One persistent RK launch over members m, member i at its chunk chunk[i]
+// (records [chunk R, ...) into snapshot buffer chunk mod 3); every member's
+// vcs must divide csh.
+int launch_rk_members(smd_ctx *ctx, const std::vector<Member *> &m, const std::vector<int> &chunk, int prec,
+                      int zt, int spt, int threads, int csh, int nclusters, size_t smem, const int2 *d_items,
+                      int n_items, int *d_queue, cudaStream_t st);
+int zt_of(int z);
+
 // CTAs per sample of a member for a sites-per-thread value: the fewest (a
 // power of two) whose share of the sites fits a CTA of the batch kernel and
 // the shared memory; 0 when none does.

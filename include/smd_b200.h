@@ -265,12 +265,20 @@ SMD_API int smd_batch_free(smd_ctx *ctx, int batch_id);
 
 /* ------------------------------------------------------------- serving */
 
-/* Job queue: a submitted job is copied, then taken in arrival order by one
- * of the context's worker lanes (SMD_SERVE_LANES, default 1), each with its
- * own streams, buffers and an equal share of the HBM budget, so with more
- * than one lane several jobs run on the device at once; each job's result
- * is that of smd_run of the job alone.  Outputs go to the host buffers given at submit, valid
- * once smd_poll returns SMD_OK. */
+/* Serving with continuous batching: a submitted job is copied and queued;
+ * one engine thread per context admits queued jobs' samples in arrival
+ * order as launch slots (24) and the context's HBM budget free up (a job
+ * larger than the budget runs in successive sample groups), and advances
+ * every admitted group with one persistent RK launch per precision per tick,
+ * each group at its own record position, stride and dt.  Spin states and each
+ * job's partial |S(q,w)|^2 sums stay resident in HBM until the job's last
+ * group lands.  A job's result does not depend on the jobs it shares launches
+ * with.  Jobs the batched kernel does not take (Lieb d-wave term, bond-list
+ * energies, impurities with couplings) run through smd_run between ticks.
+ * Outputs go to the host buffers given at submit, valid once smd_poll
+ * returns SMD_OK; smd_poll / smd_wait report the latency from submit.
+ * smd_cancel drops a job that has not started; a started job returns
+ * SMD_EBUSY and runs to completion. */
 SMD_API int smd_submit(smd_ctx *ctx, const smd_job_desc *job, const double *spins0,
                const double *window, double *spec_out, double *qss_out,
                long long *job_id);
