@@ -7,7 +7,7 @@ sample, the per-record projection onto all q, the windowed time transform
 and the sample accumulation of |S(q,w)|^2.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c2] [--no-cpu-baseline]
+                    [--workload c1|c2|c3|c4] [--no-cpu-baseline]
 
 Under torchrun every rank integrates its own 64 samples (weak scaling); the
 sample sums are added across ranks with one NCCL all-reduce per step, the
@@ -32,6 +32,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "SMD site-steps/s"
+# c4 bench sample count: 64 of the configuration's 512 samples (one wave of
+# the 1.7 GB-per-sample series; site-steps/s is per-sample intensive)
+C4_SAMPLES = 64
 UNIT = "site-steps/s"
 
 
@@ -58,6 +61,19 @@ def profile_traffic(name: str, records_per_launch: float = 0.0):
         traffic = int(round(traffic * records_per_launch / rec))
         src += f" (captured at {rec} records per launch, scaled to {records_per_launch:g})"
     return traffic, src
+
+
+def z_active(w, lat) -> int:
+    """Active neighbours per site of a workload's lattice."""
+    s = w.settings
+    return sum(lat.zn[k] for k, on in enumerate([True, s.j2_on, s.jx_on]) if on)
+
+
+DATA = {"q120": "seeded 120-degree states with Gaussian tilts",
+        "stripe": "seeded stripe states with Gaussian tilts",
+        "ferro": "seeded ferromagnetic states with Gaussian tilts",
+        "relaxed": "seeded random states relaxed by 200 local-field alignment steps, "
+                   "then Gaussian tilts"}
 
 
 def rel_l2(a, b):
@@ -134,12 +150,17 @@ class ClockSampler:
 
 # ------------------------------------------------------------- serving
 
-def serving_leg(ctx, n_jobs: int, seed: int):
-    """A bounded stream of serving-workload jobs (workloads.c5_stream) through
-    the job queue (smd_submit / smd_wait): one burst to measure the queue's
-    service capacity, then Poisson arrivals at 70 % of it; latency = submit
-    to completion as the library measures it."""
-    from classical_mc_and_smd_for_2d_heisenberg_models_b200 import smd, workloads
+def serving_leg(ctx, n_jobs: int, seed: int, fp64: bool = True):
+    """A stream of serving-workload jobs (workloads.c5_stream: five
+    geometries, N log-uniform in [256, 16384], 16-256 samples, 2^12-2^15 RK
+    steps, 1024 records, FP32 form) through the continuous-batching engine
+    (smd_submit / smd_wait).  One burst (every job queued at once) gives the
+    aggregate service rate; Poisson arrivals at 70 % of it give p50 / p99
+    latency (submit to completion, as the library measures it).  The same
+    jobs run one at a time through smd_run in the FP64 plain form give the
+    denominator of the 4x target and the FP64 spectra each served result's
+    DSSF rel-L2 is taken against."""
+    from classical_mc_and_smd_for_2d_heisenberg_models_b200 import _lib, smd, workloads
     jobs = workloads.c5_stream(n_jobs, seed)
     prepared = []
     for w in jobs:
@@ -158,11 +179,13 @@ def serving_leg(ctx, n_jobs: int, seed: int):
         return ctx.submit(lid, qid, spins, w.settings.dtm, w.n_rec, stride=w.stride,
                           precision=w.precision, fix_every=w.fix_every, win=win, imp=imp_arr)
 
-    # burst: every job queued at once; the largest latency is the makespan
+    # burst: every job queued at once; the makespan gives the service rate
+    t0 = time.perf_counter()
     ids = [submit(p) for p in prepared]
-    lat = [ctx.wait(j)[2] for j in ids]
-    makespan_ms = max(lat)
-    rate = 0.7 * len(prepared) / (makespan_ms / 1e3)
+    burst = [ctx.wait(j) for j in ids]
+    makespan = time.perf_counter() - t0
+    infos = [ctx.job_info(j) for j in ids]
+    rate = 0.7 * len(prepared) / makespan
     rng = np.random.default_rng(seed + 1)
     gaps = rng.exponential(1.0 / rate, size=len(prepared))
     t0 = time.perf_counter()
@@ -175,13 +198,31 @@ def serving_leg(ctx, n_jobs: int, seed: int):
         ids.append(submit(p))
     lat = np.array([ctx.wait(j)[2] for j in ids])
     wall = time.perf_counter() - t0
-    return {"jobs": len(prepared), "arrivals": "Poisson", "rate_jobs_per_s": rate,
-            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-            "max_ms": float(lat.max()), "burst_site_steps_per_s": site_steps / (makespan_ms / 1e3),
-            "sample": f"{len(prepared)} jobs of the serving mix (5 geometries, N log-uniform in "
-                      f"[256, 4096], 16-48 samples, 4092 RK steps at stride 4, 0-10 % vacancies, "
-                      f"grid q, FP32 form), Poisson at 70 % of the burst service rate; "
-                      f"stream wall time {wall:.1f} s"}
+    out = {"jobs": len(prepared), "arrivals": "Poisson", "rate_jobs_per_s": rate,
+           "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+           "max_ms": float(lat.max()), "site_steps": float(site_steps),
+           "burst_makespan_s": makespan, "served_site_steps_per_s": site_steps / makespan,
+           "energy_drift_per_site": {"max": max(i["drift_max"] for i in infos),
+                                     "final": max(i["drift_final"] for i in infos)},
+           "sample": f"{len(prepared)} jobs of the serving mix (5 geometries, N log-uniform in "
+                     f"[256, 16384], 16-256 samples, 2^12-2^15 RK steps at the stride giving "
+                     f"1024 records, 0-10 % vacancies, grid q, FP32 form), Poisson at 70 % of "
+                     f"the burst service rate; stream wall time {wall:.1f} s",
+           "job_shapes": [f"{w.settings.geom} N={w.settings.N} S={w.n_samples} "
+                          f"steps={w.steps}" for w, *_ in prepared]}
+    if fp64:
+        ms64, rels = 0.0, []
+        for (w, lid, qid, spins, imp_arr, win), (spec, _, _) in zip(prepared, burst):
+            r = ctx.run(lid, qid, spins, w.settings.dtm, w.n_rec, stride=w.stride,
+                        precision=_lib.SMD_FP64, fix_every=1, win=win, imp=imp_arr,
+                        want_final=False)
+            ms64 += r.report["ms_device"]
+            rels.append(rel_l2(spec, r.spec))
+        out["fp64_plain_site_steps_per_s"] = site_steps / (ms64 / 1e3)
+        out["speedup_vs_fp64_plain"] = out["served_site_steps_per_s"] / out["fp64_plain_site_steps_per_s"]
+        out["dssf_rel_l2_vs_fp64"] = {"max": float(max(rels)), "median": float(np.median(rels)),
+                                      "per_job": [float(x) for x in rels]}
+    return out
 
 
 # --------------------------------------------------------- CPU reference
@@ -350,7 +391,11 @@ def run_ours(args, w, rank, world):
     # ---- FP64 plain form on the same workload (the 4x target's denominator)
     fp64 = None
     dssf = None
-    if not args.no_fp64:
+    z = z_active(w, lat)
+    fpss = flops_per_site_step(z)
+    peak64 = C.c_double()
+    ok64 = lib.smd_measure_fma_peak(local, _lib.SMD_FP64, C.byref(peak64)) == 0
+    if not args.no_fp64 and w.precision != _lib.SMD_FP64:
         device_step(_lib.SMD_FP64, 1)
         r64 = [device_step(_lib.SMD_FP64, 1) for _ in range(max(1, min(args.steps, 2)))]
         ms64 = sum(r.ms_device for r in r64)
@@ -371,10 +416,14 @@ def run_ours(args, w, rank, world):
                 "ms_proj_per_step": sum(r.ms_proj for r in r64) / len(r64),
                 "ms_tfft_per_step": sum(r.ms_tfft for r in r64) / len(r64),
                 "drift_max_per_site": max(r.drift_max for r in r64)}
+        ach64 = fpss * site_steps_rank * len(r64) / (sum(r.ms_rk for r in r64) / 1e3) / 1e12
+        fp64["rk_roofline"] = {"kernel": "rk_cluster_kernel<double>", "bound": "fp64",
+                               "achieved": ach64, "unit": "TFLOP/s",
+                               "peak": peak64.value if ok64 else None,
+                               "frac": ach64 / peak64.value if ok64 and peak64.value > 0 else None,
+                               "peak_source": "smd_measure_fma_peak (FP64 FMA chains on every SM)"}
 
     # ---- roofline of the dominant kernel (RK4 + correction)
-    z = sum(lat.zn[k] for k, on in enumerate([True, s.j2_on, s.jx_on]) if on)
-    fpss = flops_per_site_step(z)
     peak = C.c_double()
     prec_peak = lib.smd_measure_fma_peak(local, w.precision, C.byref(peak))
     rk_flops = fpss * site_steps_rank * args.steps
@@ -403,12 +452,15 @@ def run_ours(args, w, rank, world):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32 stages / f64 master+energy",
-            "data": "synthetic (seeded 120-degree states with 0.15 rad Gaussian tilts)",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 stages / f64 master+energy" if w.precision == _lib.SMD_FP32 else "f64",
+            "data": f"synthetic ({DATA.get(w.state, w.state)}, sigma {w.sigma} rad)",
             "config": {"workload": w.describe(), "samples_per_gpu": S,
                        "rk_steps": w.steps, "records": n, "Q": Q,
                        "l2": "inputs larger than L2 (time series %.1f GB per GPU)" %
-                             (S * 3 * n * Q * 8 / 1e9),
+                             (S * 3 * n * Q * (8 if w.precision == _lib.SMD_FP32 else 16) / 1e9)
+                             if S * 3 * n * Q * 8 > 126e6 else
+                             "inputs smaller than L2 (126 MB): a latency-bound small case",
                        "parallelism": f"samples sharded over {world} GPU(s)"},
             "dssf_samples_per_s": samples_per_s,
             "breakdown_ms_per_step": {"device": ms_dev / args.steps, "rk": ms_rk / args.steps,
@@ -426,6 +478,176 @@ def run_ours(args, w, rank, world):
             "clocks": clk.summary(),
         }
     return line
+
+
+def run_batch(args, bw, rank, world):
+    """The batched form (smd_batch_*): every member lattice's samples in one
+    persistent RK launch per chunk of records, the job step replayed as one
+    CUDA graph.  One bench step = one job step of the whole batch."""
+    import torch
+    from classical_mc_and_smd_for_2d_heisenberg_models_b200 import _lib, smd, workloads
+    import ctypes as C
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = f"cuda:{local}"
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    ctx = smd.Context(local)
+    lib = ctx.lib
+    mem = []
+    for k, w in enumerate(bw.members):
+        s = w.settings
+        lat = smd.build_lattice(s.geom, s.L)
+        lid = ctx.lattice(s, lat)
+        ql = workloads.bz_points(lat, bw.n_q, w.seed + 1)
+        qid = ctx.qset(lid, use_grid=False, qlist=ql)
+        spins, imp = workloads.make_inputs(w, rank, lat=lat)
+        mem.append((w, lat, lid, qid, spins, imp, ctx.qset_size(qid)))
+    m0 = bw.members[0]
+    n = m0.n_rec
+    win = smd.window(m0.window, n)
+    b = ctx.batch([(lid, qid, w.n_samples, imp) for (w, lat, lid, qid, spins, imp, Q) in mem],
+                  m0.settings.dtm, n, m0.stride, m0.precision, m0.fix_every)
+    tuning = b.info()
+    d_in = [torch.from_numpy(x[4]).to(dev) for x in mem]
+    d_win = torch.from_numpy(win).to(dev)
+    d_spec = [torch.zeros((3, x[6], n), dtype=torch.float64, device=dev) for x in mem]
+    d_qss = [torch.zeros(n, dtype=torch.float64, device=dev) for x in mem]
+    k = len(mem)
+    VP = C.c_void_p
+    ins = (VP * k)(*[t.data_ptr() for t in d_in])
+    so = (VP * k)(*[t.data_ptr() for t in d_spec])
+    qo = (VP * k)(*[t.data_ptr() for t in d_qss])
+
+    def step():
+        rep = _lib.Report()
+        rc = lib.smd_batch_run_device(ctx.h, b.id, ins, VP(d_win.data_ptr()), so, qo, C.byref(rep))
+        if rc:
+            raise _lib.SMDError(rc, lib.smd_last_error(ctx.h).decode())
+        return rep
+
+    first = step()   # eager, with per-launch timing of the batch RK kernel
+    for _ in range(max(0, args.warmup - 1)):
+        step()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    reps = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            reps.append(step())
+        torch.cuda.synchronize()
+    ms_dev = sum(r.ms_device for r in reps)
+    t = torch.tensor([ms_dev], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    site_steps_rank = sum(float(w.settings.N) * w.n_samples * w.steps for w, *_ in mem)
+    value = site_steps_rank * world * args.steps / (ms_max / 1e3)
+    n_samples = sum(w.n_samples for w, *_ in mem)
+    spec32 = [x.cpu().numpy().copy() for x in d_spec]
+
+    # e2e: host buffers through smd_batch_run
+    pins = [torch.from_numpy(x[4]).pin_memory() for x in mem]
+    pwin = torch.from_numpy(win).pin_memory()
+    pspec = [torch.zeros((3, x[6], n), dtype=torch.float64).pin_memory() for x in mem]
+    pqss = [torch.zeros(n, dtype=torch.float64).pin_memory() for x in mem]
+    P = C.POINTER(C.c_double)
+    cp = lambda tt: C.cast(C.c_void_p(tt.data_ptr()), P)
+    hin = (P * k)(*[cp(x) for x in pins])
+    hso = (P * k)(*[cp(x) for x in pspec])
+    hqo = (P * k)(*[cp(x) for x in pqss])
+
+    def e2e():
+        rep = _lib.Report()
+        t0 = time.perf_counter()
+        rc = lib.smd_batch_run(ctx.h, b.id, hin, cp(pwin), hso, hqo, C.byref(rep))
+        t1 = time.perf_counter()
+        if rc:
+            raise _lib.SMDError(rc, lib.smd_last_error(ctx.h).decode())
+        return t1 - t0
+
+    e2e()
+    e2e_t = max(e2e() for _ in range(max(1, min(args.steps, 3))))
+    e2e_value = site_steps_rank * world / e2e_t
+
+    # FP64 plain form: every member alone through smd_run_device, FP64,
+    # correction every step (no batching): the denominator of the 4x target
+    fp64, dssf = None, None
+    if not args.no_fp64:
+        ms64, rels, rk64, ff64 = 0.0, [], 0.0, 0.0
+        for mi, ((w, lat, lid, qid, spins, imp, Q), dsp, s32) in enumerate(zip(mem, d_spec, spec32)):
+            dsp.zero_()
+            dq = torch.zeros(n, dtype=torch.float64, device=dev)
+            imp_arr = None if imp is None else np.ascontiguousarray(imp, np.int32)
+            j = ctx.job(lid, qid, w.n_samples, w.settings.dtm, n, w.stride, _lib.SMD_FP64, 1, imp_arr)
+            rep = _lib.Report()
+            torch.cuda.synchronize()
+            rc = lib.smd_run_device(ctx.h, C.byref(j), VP(d_in[mi].data_ptr()),
+                                    VP(d_win.data_ptr()), VP(dsp.data_ptr()), VP(dq.data_ptr()), None,
+                                    C.byref(rep))
+            if rc:
+                raise _lib.SMDError(rc, lib.smd_last_error(ctx.h).decode())
+            ms64 += rep.ms_device
+            rk64 += rep.ms_rk
+            ff64 += flops_per_site_step(z_active(w, lat)) * float(w.settings.N) * w.n_samples * w.steps
+            rels.append(rel_l2(s32, dsp.cpu().numpy()))
+        fp64 = {"value": site_steps_rank / (ms64 / 1e3), "unit": UNIT, "ms_per_step": ms64,
+                "ms_rk_per_step": rk64, "rk_achieved_tflops": ff64 / (rk64 / 1e3) / 1e12,
+                "form": "each lattice alone through smd_run, FP64, correction every step"}
+        dssf = {"max": float(max(rels)), "per_member": [float(x) for x in rels],
+                "reference": "FP64 plain form of each lattice on the same samples"}
+
+    # roofline of the batch RK kernel (eager first run: CUDA events around
+    # every launch on the RK stream)
+    flops = sum(flops_per_site_step(z_active(w, lat)) * float(w.settings.N) * w.n_samples * w.steps
+                for (w, lat, *_rest) in mem)
+    achieved = flops / (first.ms_rk / 1e3) / 1e12
+    peak = C.c_double()
+    okp = lib.smd_measure_fma_peak(local, m0.precision, C.byref(peak)) == 0
+    traffic, traffic_src = profile_traffic("rk_batch_kernel_c3.md")
+    roof = {"kernel": "rk_batch_kernel", "bound": "fp32" if m0.precision == _lib.SMD_FP32 else "fp64",
+            "achieved": achieved, "peak": peak.value if okp else None, "unit": "TFLOP/s",
+            "frac": achieved / peak.value if okp and peak.value > 0 else None,
+            "peak_source": "smd_measure_fma_peak (FMA chains on every SM)",
+            "algorithmic_flops_per_site_step": "42 z + 150 per member",
+            "avg_launch_ms": first.ms_rk / max(1, first.rk_launches),
+            "traffic": traffic, "traffic_unit": "bytes per launch (DRAM read + write)",
+            "traffic_source": traffic_src}
+    b.free()
+    if dist is not None:
+        dist.destroy_process_group()
+    ctx.close()
+    if rank != 0:
+        return None
+    h2d = sum(x[4].nbytes for x in mem) + win.nbytes
+    d2h = sum(3 * x[6] * n * 8 + n * 8 for x in mem)
+    return {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 stages / f64 master+energy",
+        "data": f"synthetic ({DATA['relaxed']}, sigma {m0.sigma} rad)",
+        "config": {"workload": bw.describe(), "samples_per_gpu": n_samples, "rk_steps": m0.steps,
+                   "records": n, "q_per_lattice": bw.n_q,
+                   "l2": "inputs larger than L2 (time series %.1f GB per GPU)" %
+                         (sum(w.n_samples * 3 * n * Q * 8 for (w, *_r, Q) in mem) / 1e9),
+                   "parallelism": f"samples sharded over {world} GPU(s)",
+                   "graph": "one CUDA graph launch per job step (the first, eager run is warm-up)"},
+        "dssf_samples_per_s": n_samples * world * args.steps / (ms_max / 1e3),
+        "autotuner": tuning,
+        "energy_drift_per_site": {"max": max(r.drift_max for r in reps),
+                                  "final": max(r.drift_final for r in reps)},
+        "dssf_rel_l2": dssf, "fp64_plain": fp64,
+        "speedup_vs_fp64_plain": value / fp64["value"] if fp64 else None,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": e2e_t * 1e3},
+        "roofline": roof, "gpu_launches": sum(r.kernel_launches for r in reps),
+        "clocks": clk.summary(),
+    }
 
 
 def cpu_baseline(w, args):
@@ -476,12 +698,12 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2")
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4"])
     ap.add_argument("--ref-ntm", type=int, default=1025)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
-    ap.add_argument("--serving-jobs", type=int, default=24)
+    ap.add_argument("--serving-jobs", type=int, default=12)
     ap.add_argument("--records", type=int, default=0,
                     help="override the record count (small profiling cases only)")
     ap.add_argument("--samples", type=int, default=0,
@@ -491,15 +713,23 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     from classical_mc_and_smd_for_2d_heisenberg_models_b200 import workloads
     import dataclasses
-    w = workloads.WORKLOADS[args.workload]()
-    if args.records:
-        w = dataclasses.replace(w, n_rec=args.records)
-    if args.samples:
-        w = dataclasses.replace(w, n_samples=args.samples)
+    if args.workload == "c3":
+        bw = workloads.c3(args.samples or 256)
+        # the reference arm and the CPU baseline run the batch's largest lattice
+        w = max(bw.members, key=lambda m: m.settings.N)
+    else:
+        bw = None
+        w = workloads.WORKLOADS[args.workload]()
+        if args.workload == "c4" and not args.samples:
+            w = dataclasses.replace(w, n_samples=C4_SAMPLES)
+        if args.records:
+            w = dataclasses.replace(w, n_rec=args.records)
+        if args.samples:
+            w = dataclasses.replace(w, n_samples=args.samples)
     if args.impl == "reference":
         line = run_reference_arm(args, w, rank, world)
     else:
-        line = run_ours(args, w, rank, world)
+        line = run_batch(args, bw, rank, world) if bw is not None else run_ours(args, w, rank, world)
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(w, args)
     if rank == 0 and line is not None:

@@ -28,6 +28,7 @@ EXPORTS = [
     "smd_lattice_sites", "smd_run", "smd_run_device", "smd_dyn_spectrum_ref",
     "smd_evolve", "smd_batch_create", "smd_batch_info", "smd_batch_run",
     "smd_batch_run_device", "smd_batch_free", "smd_submit", "smd_poll", "smd_wait", "smd_cancel",
+    "smd_job_info",
     "smd_serve_shutdown", "smd_evolve_fp64_noalloc", "smd_measure_fma_peak",
 ]
 
@@ -137,6 +138,7 @@ def load():
     L.smd_poll.argtypes = [vp, C.c_longlong, dp]
     L.smd_wait.argtypes = [vp, C.c_longlong, C.c_double, dp]
     L.smd_cancel.argtypes = [vp, C.c_longlong]
+    L.smd_job_info.argtypes = [vp, C.c_longlong, C.POINTER(Report)]
     L.smd_serve_shutdown.argtypes = [vp]
     L.smd_serve_shutdown.restype = None
     L.smd_evolve_fp64_noalloc.argtypes = [C.POINTER(NoAllocModel), C.c_int, C.c_double, C.c_int,

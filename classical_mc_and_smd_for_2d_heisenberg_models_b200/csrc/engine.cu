@@ -36,6 +36,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <condition_variable>
 #include <cstdlib>
 #include <cstring>
@@ -80,14 +81,16 @@ struct SJob {
     int next_sample = 0, groups_live = 0, vcs = 1, R = 0;
     size_t acc_bytes = 0;
     DevBuf acc, accq, win, stat;
-    Pinned *stage = nullptr;
+    Pinned *stage = nullptr;       // spectra, autocorrelation, status, then [n_samples][4] energy stats
     cudaEvent_t ev_out = nullptr;
+    double drift_max = 0.0, drift_final = 0.0;
 };
 
 struct Group {
     std::unique_ptr<Member> m;
     SJob *job = nullptr;
     int chunk = 0;
+    int s_begin = 0;   // first sample of the job in this group
     size_t bytes = 0;
 };
 
@@ -195,6 +198,9 @@ int Engine::start_job(SJob &j)
     CK(cudaMemsetAsync(j.stat.p, 0, sizeof(int), st), "memset");
     CK(cudaMemcpyAsync(j.win.p, j.window.data(), n * 8, cudaMemcpyHostToDevice, st), "H2D window");
     CK(cudaEventCreateWithFlags(&j.ev_out, cudaEventDisableTiming), "event");
+    // staging for the outputs and every sample's energy statistics
+    j.stage = get_pinned((3 * Q * n + n) * 8 + 64 + (size_t)j.desc.n_samples * 32);
+    if (!j.stage) return fail(ctx, SMD_ECUDA, "serving: pinned staging");
     used += j.acc_bytes;
     return SMD_OK;
 }
@@ -299,6 +305,7 @@ int Engine::admit()
                 j.accq.release();
                 j.win.release();
                 j.stat.release();
+                if (j.stage) j.stage->busy = false;
                 used -= j.acc_bytes;
                 set_error("job " + std::to_string(j.id) + ": one sample exceeds the HBM budget");
                 j.status = SMD_ENOMEM_ADMIT;
@@ -331,6 +338,7 @@ int Engine::admit()
             done_cv.notify_all();
             if (j.groups_live == 0) {
                 running.erase(std::find(running.begin(), running.end(), jp));
+                if (j.stage) j.stage->busy = false;
                 used -= j.acc_bytes;
             }
             continue;
@@ -344,6 +352,7 @@ int Engine::admit()
         Group g;
         g.m = std::move(m);
         g.job = &j;
+        g.s_begin = j.next_sample;
         g.bytes = bytes;
         used += bytes;
         j.next_sample += S;
@@ -416,6 +425,10 @@ int Engine::do_tick()
             SJob &j = *g.job;
             rc = member_finish(ctx, m, j.acc.as<double>(), j.accq.as<double>(), spr, &launches);
             if (rc) return rc;
+            // the group's energy statistics ([S][4]: max drift, last E, E0, -)
+            const size_t Q = j.Qs->Q, n = j.desc.n_rec;
+            char *h = static_cast<char *>(j.stage->p) + (3 * Q * n + n) * 8 + 64 + (size_t)g.s_begin * 32;
+            CK(cudaMemcpyAsync(h, m.stats.p, (size_t)m.S * 32, cudaMemcpyDeviceToHost, spr), "D2H stats");
         }
     }
     CK(cudaEventRecord(ev_proj[bt], spr), "event");
@@ -443,8 +456,6 @@ int Engine::do_tick()
             // the job's averages to pinned staging
             const size_t Q = j.Qs->Q, n = j.desc.n_rec, ns = 3 * Q * n;
             const double fc = 1.0 / (double)j.desc.n_samples;   // smd_code.cpp:3596-3611
-            j.stage = get_pinned((ns + n) * 8 + sizeof(int));
-            if (!j.stage) return fail(ctx, SMD_ECUDA, "serving: pinned staging");
             CK(launch_scale(j.acc.as<double>(), ns, fc, spr), "scale");
             CK(launch_scale(j.accq.as<double>(), n, fc, spr), "scale");
             char *h = static_cast<char *>(j.stage->p);
@@ -475,6 +486,12 @@ void Engine::reap()
         std::memcpy(j.qss_out, h + ns * 8, n * 8);
         int st = 0;
         std::memcpy(&st, h + (ns + n) * 8, sizeof(int));
+        const double *stt = reinterpret_cast<const double *>(h + (ns + n) * 8 + 64);
+        const double N = (double)j.L->N;
+        for (int k = 0; k < j.desc.n_samples; k++) {
+            j.drift_max = std::max(j.drift_max, stt[4 * k] / N);
+            j.drift_final = std::max(j.drift_final, std::fabs(stt[4 * k + 1] - stt[4 * k + 2]) / N);
+        }
         j.stage->busy = false;
         int rc = SMD_OK;
         if (st & 4) rc = SMD_ETIMEOUT;
@@ -695,4 +712,23 @@ extern "C" int smd_cancel(smd_ctx *ctx, long long job_id)
     if (j.started) return SMD_EBUSY;   // samples already on the device run to completion
     j.cancelled = true;
     return SMD_OK;
+}
+
+extern "C" int smd_job_info(smd_ctx *ctx, long long job_id, smd_report *rep)
+{
+    if (!ctx || !rep) return SMD_EINVAL;
+    Engine *e = engine_for(ctx);
+    std::lock_guard<std::mutex> lk(e->mu);
+    auto it = e->jobs.find(job_id);
+    if (it == e->jobs.end()) return SMD_ENOTFOUND;
+    SJob &j = *it->second;
+    if (j.status == SMD_EBUSY) return SMD_EBUSY;
+    std::memset(rep, 0, sizeof *rep);
+    rep->ms_total = std::chrono::duration<double, std::milli>(j.t_done - j.t_submit).count();
+    rep->site_steps = 0.0;
+    if (j.L) rep->site_steps = (double)j.L->N * (double)(j.desc.n_rec - 1) * j.desc.stride * j.desc.n_samples;
+    rep->drift_max = j.drift_max;
+    rep->drift_final = j.drift_final;
+    rep->rk_kind = j.batched ? 3 : 1;
+    return j.status;
 }

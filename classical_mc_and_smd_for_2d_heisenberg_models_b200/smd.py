@@ -323,6 +323,14 @@ class Context:
         spec, qss = self._keep.pop(("job", job_id))
         return spec, qss, lat.value
 
+    def job_info(self, job_id: int) -> dict:
+        """Latency, site-steps and energy drift of a finished job."""
+        rep = _lib.Report()
+        rc = self.lib.smd_job_info(self.h, job_id, C.byref(rep))
+        if rc:
+            raise SMDError(rc, f"job {job_id}")
+        return {k: getattr(rep, k) for k, _ in _lib.Report._fields_}
+
     def poll(self, job_id: int) -> int:
         lat = C.c_double()
         return self.lib.smd_poll(self.h, job_id, C.byref(lat))

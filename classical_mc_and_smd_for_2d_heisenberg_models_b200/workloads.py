@@ -13,9 +13,14 @@ precision form, and the q points.
       0.15 rad tilts, FP32 precision form, dt=0.02, stride 4, 4096 records
       (2048 positive frequencies), FP64 correction every 16 steps,
       48 x 48 grid + 512-point Gamma-K-M-Gamma path
+  c3  batch of seven lattices of uneven N (square L=24..64, kagome 24,
+      honeycomb 30, Lieb 32), 5% vacancies, 256 samples, relaxed random
+      states, FP32, 8192 steps, 4096 random first-BZ q per lattice
   c4  square L=128 (N=16384), J2=0.55 J3=0.1 lambda=0.9 h=0.3, 5% vacancies,
       512 samples, stripe with 0.1 rad tilts, FP32, dt=0.01, stride 8,
       4096 records, 128 x 128 grid + 1024-point path
+  c5  serving stream (c5_stream): five geometries, N log-uniform in
+      [256, 16384], 16-256 samples, 2^12-2^15 steps
 The number of RK steps of a job is (records - 1) * stride.
 """
 from __future__ import annotations
@@ -101,6 +106,109 @@ def c4(n_samples: int = 512) -> Workload:
     return Workload("c4", s, n_samples, "stripe", 0.1, 8, 4096, SMD_FP32, 16, 1024, 0x5eed04)
 
 
+@dataclasses.dataclass
+class BatchWorkload:
+    """Several lattices run as one batch (smd_batch_*): one Workload per
+    member, all with the same dt, records, stride and precision form."""
+    name: str
+    members: list
+    n_q: int
+
+    @property
+    def steps(self) -> int:
+        return self.members[0].steps
+
+    def describe(self) -> str:
+        parts = [f"{w.settings.geom} L={w.settings.L} (N={w.settings.N}, J2={w.settings.J2:.3f}, "
+                 f"{w.n_samples} samples)" for w in self.members]
+        m0 = self.members[0]
+        return (f"{self.name}: batch of {len(self.members)} lattices [" + "; ".join(parts) +
+                f"], 5% vacancies each, {sum(w.n_samples for w in self.members)} samples, "
+                f"{m0.steps} RK4 steps (stride {m0.stride}, {m0.n_rec} records), "
+                f"{'FP64 plain' if m0.precision == SMD_FP64 else 'FP32 precision form'}, "
+                f"{self.n_q} random first-BZ q per lattice")
+
+
+def bz_points(lat, n: int, seed: int) -> np.ndarray:
+    """n points drawn uniformly in the first Brillouin zone of the lattice's
+    Bravais lattice (the Wigner-Seitz cell of its reciprocal lattice), in
+    the frame of the lattice's grid positions."""
+    g1, g2 = lat.grid_basis()
+    b1, b2 = g1 * lat.G / lat.grid_fac, g2 * lat.G / lat.grid_fac   # reciprocal of the Bravais cell
+    rng = np.random.default_rng(seed)
+    u = rng.uniform(0.0, 1.0, size=(n, 2))
+    q = u[:, :1] * b1 + u[:, 1:] * b2
+    best = q.copy()
+    for n1 in (-2, -1, 0, 1, 2):
+        for n2 in (-2, -1, 0, 1, 2):
+            c = q - (n1 * b1 + n2 * b2)
+            better = np.linalg.norm(c, axis=1) < np.linalg.norm(best, axis=1)
+            best[better] = c[better]
+    return best
+
+
+def relaxed_samples(s: SMDSettings, lat, n_samples: int, sweeps: int, sigma: float, seed: int):
+    """Random unit vectors relaxed toward a ground state by `sweeps` damped
+    local-field alignment steps S_i <- normalise(S_i - eta h_i) (vectorised
+    over sites and samples, FP64), then tilted by Gaussian tangent vectors of
+    width sigma.  Vacancies feel no exchange field and keep their random
+    spin.  Returns (spins [n][N][3], imp [n][N] or None)."""
+    from . import samples as smp
+    rng = np.random.default_rng(seed)
+    N = lat.N
+    S = rng.normal(size=(n_samples, N, 3))
+    S /= np.linalg.norm(S, axis=2, keepdims=True)
+    imp = None
+    if s.disorder:
+        imp = np.stack([smp.impurity_map(N, s.imp_ratio, rng) for _ in range(n_samples)])
+    J = [s.J1, s.J2, s.JX]
+    on = [True, s.j2_on, s.jx_on]
+    lam = np.array(s.lambdas())
+    mask = None if imp is None else (1.0 - imp)[:, :, None]
+    eta = 0.5 / max(1e-12, sum(abs(J[k]) * lat.zn[k] for k in range(3) if on[k]))
+    for _ in range(sweeps):
+        Sm = S if mask is None else S * mask
+        h = np.zeros_like(S)
+        for k in range(3):
+            if not on[k] or lat.zn[k] == 0:
+                continue
+            nb = lat.nbrs[k]
+            for e in range(lat.zn[k]):
+                j = nb[:, e]
+                ok = (j >= 0)[None, :, None]
+                h += J[k] * lam[k][None, None, :] * np.where(ok, Sm[:, np.clip(j, 0, None), :], 0.0)
+        if mask is not None:
+            h *= mask
+        h[:, :, 2] -= s.h
+        S = S - eta * h
+        S /= np.linalg.norm(S, axis=2, keepdims=True)
+    out = np.stack([smp.tilt(S[k], sigma, rng) for k in range(n_samples)])
+    return out, imp
+
+
+def c3(n_samples: int = 256) -> BatchWorkload:
+    """Batched uneven mix: square L in {24, 32, 48, 64}, kagome L=24
+    (N=1728), honeycomb L=30 (N=1800; the reference's honeycomb needs L a
+    multiple of 6, so L=32 is not buildable) and Lieb L=32 (N=2048: the
+    reference's Lieb cell has 2 sites, not 3), 5% vacancies each, J1=1, J2
+    drawn in [0, 0.8] per lattice, lambda=1; the samples split evenly over
+    the seven lattices; 8192 RK steps (2048 records at stride 4) in the FP32
+    form with FP64 correction every 16 steps; 4096 random first-BZ q per
+    lattice."""
+    rng = np.random.default_rng(0x5eed03)
+    lats = [("square", 24), ("square", 32), ("square", 48), ("square", 64), ("kagome", 24),
+            ("hexagn", 30), ("lieb", 32)]
+    per = [n_samples // len(lats) + (1 if k < n_samples % len(lats) else 0) for k in range(len(lats))]
+    members = []
+    for k, ((geom, L), ns) in enumerate(zip(lats, per)):
+        J2 = float(rng.uniform(0.0, 0.8))
+        s = SMDSettings(geom=geom, L=L, J1=1.0, J2=J2, imp_ratio=0.05, dtm=0.01, ntm=2048,
+                        NMeas=1000 * ns)
+        members.append(Workload(f"c3_{geom}{L}", s, ns, "relaxed", 0.1, 4, 2048, SMD_FP32, 16, 0,
+                                0x5eed03 + 17 * k))
+    return BatchWorkload("c3", members, 4096)
+
+
 WORKLOADS = {"c1": c1, "c2": c2, "c4": c4}
 
 C5_GEOMS = ("square", "triang", "hexagn", "kagome", "lieb")
@@ -125,15 +233,14 @@ def _valid_L(geom: str, n_target: float, n_max: int) -> Optional[int]:
     return best
 
 
-def c5_stream(n_jobs: int, seed: int, n_min: int = 256, n_max: int = 4096,
-              samples=(16, 48), steps: int = 4096, stride: int = 4):
+def c5_stream(n_jobs: int, seed: int, n_min: int = 256, n_max: int = 16384,
+              samples=(16, 256), log2_steps=(12, 15), n_rec: int = 1024):
     """Jobs of the serving workload: lattice drawn uniformly from the five
     crystal types, N log-uniform in [n_min, n_max] snapped to a valid L,
     J1 = 1, J2 in [0, 0.8], JX in [0, 0.2], lambda in [0.8, 1.0], h in
-    [0, 0.5], 0-10 % vacancies, seeded ordered states with Gaussian tilts,
-    grid q, FP32 form.  (The full configuration reaches N = 16384, 256
-    samples and 2^15 steps; bench.py bounds N, samples and steps so the
-    stream fits a few seconds.)  Returns [(Workload, imp ratio)]."""
+    [0, 0.5], 0-10 % vacancies, 16-256 samples, 2^12-2^15 RK steps
+    (log-uniform) recorded at the stride that gives n_rec records, seeded
+    ordered states with Gaussian tilts, grid q, FP32 form."""
     rng = np.random.default_rng(seed)
     jobs = []
     states = {"square": "stripe", "triang": "q120"}
@@ -143,21 +250,29 @@ def c5_stream(n_jobs: int, seed: int, n_min: int = 256, n_max: int = 4096,
         if L is None:
             continue
         lam = float(rng.uniform(0.8, 1.0))
+        steps = int(round(2.0 ** rng.uniform(log2_steps[0], log2_steps[1])))
+        stride = max(1, steps // n_rec)
         s = SMDSettings(geom=geom, L=L, J1=1.0, J2=float(rng.uniform(0.0, 0.8)),
                         JX=float(rng.uniform(0.0, 0.2)), zlamb1=lam, zlamb2=lam,
                         h=float(rng.uniform(0.0, 0.5)), imp_ratio=float(rng.uniform(0.0, 0.1)),
-                        dtm=0.01, ntm=steps // stride)
+                        dtm=0.01, ntm=n_rec)
         n = int(rng.integers(samples[0], samples[1] + 1))
         s = dataclasses.replace(s, NMeas=1000 * n)
         w = Workload(f"c5_{len(jobs)}", s, n, states.get(geom, "ferro"), 0.1, stride,
-                     steps // stride, SMD_FP32, 16, 0, seed + 101 * len(jobs))
+                     n_rec, SMD_FP32, 16, 0, seed + 101 * len(jobs))
         jobs.append(w)
     return jobs
 
 
-def make_inputs(w: Workload, rank: int = 0):
+def make_inputs(w: Workload, rank: int = 0, lat=None):
     """Samples (and per-sample impurity maps) for one rank."""
     from . import samples as smp
+    if w.state == "relaxed":
+        if lat is None:
+            from .smd import build_lattice
+            lat = build_lattice(w.settings.geom, w.settings.L)
+        spins, imp = relaxed_samples(w.settings, lat, w.n_samples, 200, w.sigma, w.seed + 7919 * rank)
+        return spins, (None if imp is None else imp.astype(np.int32))
     spins, imp = smp.make_samples(w.settings, w.n_samples, w.state, w.sigma, w.seed + 7919 * rank)
     imp_per_sample = None
     if imp is not None:

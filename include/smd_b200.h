@@ -285,6 +285,11 @@ SMD_API int smd_submit(smd_ctx *ctx, const smd_job_desc *job, const double *spin
 SMD_API int smd_poll(smd_ctx *ctx, long long job_id, double *latency_ms);
 SMD_API int smd_wait(smd_ctx *ctx, long long job_id, double timeout_ms, double *latency_ms);
 SMD_API int smd_cancel(smd_ctx *ctx, long long job_id);
+/* Report of a finished job: latency (ms_total), site_steps, and the energy
+ * drift per site over its samples (drift_max, drift_final); rk_kind 3 when
+ * it ran in the shared launches.  Returns the job's status (SMD_EBUSY while
+ * it runs). */
+SMD_API int smd_job_info(smd_ctx *ctx, long long job_id, smd_report *rep);
 /* Stop the context's serving worker after the queued jobs (call before
  * smd_ctx_destroy when smd_submit was used). */
 SMD_API void smd_serve_shutdown(smd_ctx *ctx);
