@@ -1,4 +1,6 @@
-"""Process-level drop-in for the SMD part of the reference's xSMD_run.
+"""Process-level drop-in for the SMD part of the reference's xSMD_run (Python
+mirror of the C++ program csrc/xsmd.cpp, which also writes the text
+spectra).
 
     python -m classical_mc_and_smd_for_2d_heisenberg_models_b200.xsmd WORKDIR
         [--device D] [--precision fp64|fp32] [--stride S] [--fix-every F]
@@ -74,10 +76,12 @@ def write_corr_dat(path: str, dtm: float, qss: np.ndarray) -> None:
 
 def _window(s: SMDSettings, workdir: str) -> np.ndarray:
     if s.window == "wread":
+        # the file's values rescaled by their maximum (smd_code.cpp:2828-2848)
         w = np.fromfile(os.path.join(workdir, "outBin", "winvec.bin"), dtype=np.float64)
-        if w.size != s.ntm:
+        if w.size < s.ntm:
             raise SettingsError(f"winvec.bin holds {w.size} values, ntm = {s.ntm}")
-        return w
+        w = w[:s.ntm]
+        return (1.0 / w.max()) * w
     return smd.window(s.window, s.ntm)
 
 

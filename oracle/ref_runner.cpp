@@ -19,8 +19,13 @@
  *   sample loop     file read, checks, get_dynSpectrum, accumulation
  *                                             smd_code.cpp:3079-3291
  *
+ *   output stage    (--outputs) sample averages, MC_Bin_SpecData, window
+ *                   files, quantum-corrected zz spectra, centred slices, the
+ *                   path and cut files            smd_code.cpp:2808-2983,
+ *                                                 3596-3631, 3645-4130
+ *
  * Usage: smd_ref_run WORKDIR SAMPLES_FILE FIRST COUNT [--dump-final]
- *        [--no-dwf-guard] [--threads-note N]
+ *        [--no-dwf-guard] [--outputs]
  * WORKDIR holds the six Settings_*.txt files and receives:
  *   ref_lattice.bin  tables built by the reference (layout below)
  *   ref_spec.bin     sum over the processed samples of Sqx/Sqy/Sqz rows
@@ -87,11 +92,12 @@ int main(int argc, char **argv)
     const string samples = argv[2];
     const long first = atol(argv[3]);
     const long count = atol(argv[4]);
-    bool dump_final = false, dwf_guard = true;
+    bool dump_final = false, dwf_guard = true, outputs = false;
     for (int a = 5; a < argc; a++) {
         string s = argv[a];
         if (s == "--dump-final") dump_final = true;
         if (s == "--no-dwf-guard") dwf_guard = false;
+        if (s == "--outputs") outputs = true;
     }
     if (chdir(workdir.c_str()) != 0) {
         cerr << "cannot enter " << workdir << "\n";
@@ -139,7 +145,6 @@ int main(int argc, char **argv)
     npt = tpLstSz;
     double Temp = Temp1;
     if (npt > 1) Temp = Temp1 + tpIndex * (Temp2 - Temp1) / (npt - 1);
-    (void)Temp;
 
     dSFMT_init(20240601);
 
@@ -318,6 +323,147 @@ int main(int argc, char **argv)
             put(f, &accz[(size_t)k * ntm], ntm);
         }
         put(f, accq.data(), ntm);
+    }
+    if (outputs) {
+        /* The root's output stage, calling the reference's own functions:
+           sample averages (smd_code.cpp:3596-3611), their binary record
+           (3613-3631), the window files (2895-2983), the quantum correction
+           of the zz spectra (3645-3670; x and y are left as they are, the
+           reference's xy/yz/tt values being undefined), centred slices
+           (3813-3855), path and cut files (3700-3735, 3996-4130) and the
+           autocorrelation (4019-4033). */
+        ostringstream oss0;
+        oss0 << fixed << setprecision(5) << Temp;
+        const string tTagDat = "_T(" + oss0.str() + ")" + outLabel + ".dat";
+        const string tTagBin = "_T(" + oss0.str() + ")" + outLabel + ".bin";
+        mkdir("outData", 0755);
+        mkdir("outData/RK_Check", 0755);
+        mkdir("outData/MC_Results", 0755);
+        mkdir("outData/RK_Results", 0755);
+        const double fc = 1.0 / count;
+        for (int k = 0; k < Nq; k++)
+            for (int n = 0; n < ntm; n++) {
+                SqxWVec[k][n] = fc * accx[(size_t)k * ntm + n];
+                SqyWVec[k][n] = fc * accy[(size_t)k * ntm + n];
+                SqzWVec[k][n] = fc * accz[(size_t)k * ntm + n];
+            }
+        for (int n = 0; n < ntm; n++) qSStVec[n] = fc * accq[n];
+        {
+            ofstream f(outDir0 + "MC_Bin_SpecData" + tTagBin, ios::binary);
+            for (int k = 0; k < Nq; k++) {
+                put(f, SqxWVec[k], ntm);
+                put(f, SqyWVec[k], ntm);
+                put(f, SqzWVec[k], ntm);
+            }
+            put(f, qSStVec, ntm);
+        }
+        {
+            ofstream recWin1(outDir1 + "RK_Check/0WinTVec_" + tWForm + ".dat");
+            ofstream recWin2(outDir1 + "RK_Check/0WinSpec_" + tWForm + ".dat");
+            complex<double> *twvec = new complex<double>[ntm];
+            prepare_wPlan_fftw1D();
+            for (int n = 0; n < ntm; n++) twvec[n] = complex<double>(tmWinVec[n], 0.0);
+            set_Input_fftw1D(twvec);
+            double *wvec0 = new double[ntm], *wvec1 = new double[ntm];
+            fftw_execute(wPlan);
+            for (int n = 0; n < ntm; n++) {
+                complex<double> wc(wfData[n][0], wfData[n][1]);
+                wvec0[n] = (1.0 / ntm) * real(wc * conj(wc));
+            }
+            get_OrderedSpecArray1D(wvec0, wvec1);
+            double wref = wvec1[0];
+            for (int n = 1; n < ntm; n++)
+                if (wvec1[n] > wref) wref = wvec1[n];
+            const double fs0 = 2.0 / ntm;
+            for (int n = 0; n < ntm; n++) {
+                recWin1 << n * dtm << X3 << tmWinVec[n] << endl;
+                recWin2 << n * fs0 - 1.0 << X3 << log10(wvec1[n] / wref) << endl;
+            }
+            destroy_wPlan_fftw1D();
+            delete[] twvec;
+            delete[] wvec0;
+            delete[] wvec1;
+        }
+        /* dq and the path length npPath as main sets them
+           (smd_code.cpp:1774-1791) */
+        dq = pi2 / Gsz;
+        {
+            vector<Vec2d> bw;
+            int n1 = 0;
+            get_qPathWVectors(n1, bw);
+            npPath = n1;
+        }
+        const double Beta = 1.0 / Temp;
+        const double itFac = tmax / pi2;
+        for (int k = 0; k < Nq; k++) {
+            double qtFac = 1.0;
+            for (int n = 0; n < ntm; n++) {
+                const double wfreq = n * dwf, f2 = Beta * wfreq;
+                if (n > 0) qtFac = f2 / (1.0 - exp(-f2));
+                SqzWVec[k][n] = itFac * qtFac * SqzWVec[k][n];
+            }
+        }
+        const int npw = ntm / 2, nmax = npw;
+        double *zzSpecPath = new double[npPath];
+        double **zzSpPathWVec = Alloc_dble_array(npPath, npw);
+        double **specField = Alloc_dble_array(Nq, 3);
+        double **xyA = Alloc_dble_array(Gsz, Gsz), **yzA = Alloc_dble_array(Gsz, Gsz);
+        double **zzA = Alloc_dble_array(Gsz, Gsz), **ttA = Alloc_dble_array(Gsz, Gsz);
+        const int nwSkip = ceil(0.1 * nmax);
+        ostringstream wOss;
+        for (int n = 0; n < npw; n++) {
+            for (int k = 0; k < Nq; k++) {
+                specField[k][0] = SqxWVec[k][n];
+                specField[k][1] = SqyWVec[k][n];
+                specField[k][2] = SqzWVec[k][n];
+            }
+            get_OrderedSpecArray2D(specField, xyA, yzA, zzA, ttA);
+            get_Spec_qPath(zzA, zzSpecPath);
+            for (int j = 0; j < npPath; j++) zzSpPathWVec[j][n] = zzSpecPath[j];
+            if (n % nwSkip == 0) {
+                wOss << fixed << setprecision(3) << n * dwf;
+                record_SpecArray2D(zzA, "DFT_zzSpec_wfreq(" + wOss.str() + ")" + tTagDat, 1);
+                wOss.str("");
+            }
+        }
+        {
+            ofstream f(outDir1 + subDir1 + "SpinSpin_Temporal_Corr" + tTagDat);
+            for (int n = 0; n < ntm; n++)
+                f << fmtDbleSci(n * dtm, 8, 15) << X4 << fmtDbleSci(qSStVec[n], 12, 22) << endl;
+        }
+        vector<Vec2d> bwvecPath;
+        int n0 = 0;
+        get_qPathWVectors(n0, bwvecPath);
+        double *pathLPos = new double[npPath];
+        {
+            Vec2d wref = bwvecPath[0];
+            double w0 = 0.0;
+            for (int k = 0; k < npPath; k++) {
+                Vec2d wvec = bwvecPath[k];
+                const double qx = wvec[0] - wref[0], qy = wvec[1] - wref[1];
+                w0 = w0 + sqrt(pow(qx, 2) + pow(qy, 2));
+                pathLPos[k] = w0;
+                wref = wvec;
+            }
+        }
+        const bool sq = (geom == "square") || (geom == "lieb");
+        const string p3 = (sq ? "YGMXG" : "KGMYG") + string("_wDepn_DFT_zzSpec") + tTagDat;
+        const string p5 = (sq ? "YGMCut" : "KGMCut") + string("_wDepn_DFT_zzSpec") + tTagDat;
+        const double cut1 = sq ? pi * 0.5 : 0.0, cut2 = sq ? pi * (1.0 + 0.5 * sq2) : pi;
+        ofstream o3(outDir1 + subDir2 + p3), o5(outDir1 + subDir2 + p5);
+        for (int k = 0; k < npPath; k++) {
+            const double lpVal = pathLPos[k];
+            for (int n = 0; n < nmax; n++) {
+                const double wfreq = n * dwf, zzVal = zzSpPathWVec[k][n];
+                o3 << fmtDbleSci(lpVal, 8, 15) << X4 << fmtDbleSci(wfreq, 8, 15) << X4
+                   << fmtDbleSci(zzVal, 12, 22) << endl;
+                if ((lpVal >= cut1) && (lpVal <= cut2))
+                    o5 << fmtDbleSci(lpVal, 8, 15) << X4 << fmtDbleSci(wfreq, 8, 15) << X4
+                       << fmtDbleSci(zzVal, 12, 22) << endl;
+            }
+            o3 << endl;
+            o5 << endl;
+        }
     }
     DftiFreeDescriptor(&handle);
     printf("{\"samples\": %ld, \"Ns\": %d, \"ntm\": %d, \"Nq\": %d, "

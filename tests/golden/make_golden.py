@@ -11,8 +11,12 @@ grid map, neighbour tables, bond list), the input samples and impurity map,
 the reference's final spins after ntm - 1 RK steps, and the reference's sums
 over samples of |S(q,w)|^2 and of the autocorrelation.
 
+Spectrum cases also get text_<name>.npz: the reference's output stage
+(sample averages, window files, quantum-corrected zz slices, path and cut
+files, autocorrelation) through smd_ref_run --outputs.
+
 Run from the repository root (needs the reference sources at build time):
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref && python tests/golden/make_golden.py [--text]
 """
 from __future__ import annotations
 
@@ -93,13 +97,51 @@ def run_case(name, over, ntm, n, kind, sigma, seed, workroot):
     return info
 
 
+def run_text_case(name, over, ntm, n, kind, sigma, seed, workroot):
+    """The reference's output stage on a spectrum case (smd_ref_run
+    --outputs): its MC_Bin_SpecData, window files, autocorrelation and every
+    zz text file (slices, path, cut), stored as text_<name>.npz."""
+    import subprocess
+    s = SMDSettings(ntm=ntm, NMeas=1000 * max(n, 2), crSkip=1000, **over)
+    wd = os.path.join(workroot, "text_" + name)
+    s.write(wd)
+    pack = s.pack_size
+    total = n if not s.disorder else pack * ((n + pack - 1) // pack)
+    if not s.disorder and total not in (1,) and total % pack:
+        total = pack * ((total + pack - 1) // pack)
+    spins, imp = smp.make_samples(s, total, kind, sigma, seed)
+    path = os.path.join(wd, "samples.bin")
+    smp.write_sample_file(path, s, spins, imp)
+    r = subprocess.run([os.path.join(ROOT, "oracle", "_ref", "smd_ref_run"), wd, path, "0", str(n),
+                        "--no-dwf-guard", "--outputs"], capture_output=True, text=True)
+    if r.returncode:
+        raise RuntimeError(r.stderr)
+    files = {}
+    for sub in ("outData", "outBin"):
+        for root, _, names in os.walk(os.path.join(wd, sub)):
+            for f in names:
+                if f == "nborsList.bin":
+                    continue
+                rel = os.path.relpath(os.path.join(root, f), wd)
+                files[rel] = open(os.path.join(root, f), "rb").read()
+    np.savez_compressed(os.path.join(HERE, f"text_{name}.npz"),
+                        settings=json.dumps(dataclasses.asdict(s)),
+                        names=np.array(sorted(files)),
+                        **{f"f{i}": np.frombuffer(files[k], np.uint8) for i, k in enumerate(sorted(files))})
+    return len(files)
+
+
 def main():
     if not O.reference_available():
         raise SystemExit("oracle/_ref/smd_ref_run is missing: run `make -C oracle ref` first")
+    text_only = "--text" in sys.argv
     with tempfile.TemporaryDirectory() as tmp:
         for c in CASES:
-            info = run_case(*c, tmp)
-            print(c[0], info)
+            if not text_only:
+                info = run_case(*c, tmp)
+                print(c[0], info)
+            if c[0].startswith("spec_"):
+                print("text", c[0], run_text_case(*c, tmp), "files")
 
 
 if __name__ == "__main__":
