@@ -25,7 +25,10 @@ def load_golden(name):
 
 
 def golden_names(prefix=""):
-    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, prefix + "*.npz")))
+    """Fixture names with the prefix; without one, the trajectory and
+    spectrum cases (the text_ output-stage fixtures have another layout)."""
+    names = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, prefix + "*.npz")))
+    return names if prefix else [n for n in names if not n.startswith("text_")]
 
 
 @pytest.fixture(scope="session")
