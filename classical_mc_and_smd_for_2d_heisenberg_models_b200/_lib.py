@@ -26,7 +26,7 @@ EXPORTS = [
     "smd_geometry_info", "smd_build_lattice", "smd_build_bonds", "smd_window",
     "smd_lattice_upload", "smd_lattice_free", "smd_qset_upload", "smd_qset_size",
     "smd_lattice_sites", "smd_run", "smd_run_device", "smd_dyn_spectrum_ref",
-    "smd_evolve", "smd_batch_create", "smd_batch_info", "smd_batch_run",
+    "smd_static_prepass", "smd_evolve", "smd_batch_create", "smd_batch_info", "smd_batch_run",
     "smd_batch_run_device", "smd_batch_free", "smd_submit", "smd_poll", "smd_wait", "smd_cancel",
     "smd_job_info",
     "smd_serve_shutdown", "smd_evolve_fp64_noalloc", "smd_measure_fma_peak",
@@ -125,6 +125,8 @@ def load():
     L.smd_run_device.argtypes = [vp, C.POINTER(JobDesc), vp, vp, vp, vp, vp, C.POINTER(Report)]
     L.smd_dyn_spectrum_ref.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.c_int, dp, dp, ip,
                                        dp, dp, dp, dp]
+    L.smd_static_prepass.argtypes = [vp, C.c_int, C.c_int, C.c_int, dp, ip, dp,
+                                     C.POINTER(C.c_longlong), dp]
     L.smd_evolve.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, ip,
                              dp, C.POINTER(Report)]
     L.smd_batch_create.argtypes = [vp, C.POINTER(BatchDesc), ip]

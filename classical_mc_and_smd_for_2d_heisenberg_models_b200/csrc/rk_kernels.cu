@@ -816,6 +816,51 @@ int rk_max_sites(int precision)
     return n;
 }
 
+// ------------------------------------------------ local-field histograms
+
+// Histogram of the three components of every site's local field over S
+// samples (the static pre-pass of Codes_Folder/smd_code.cpp:2456-2480):
+// bin round((h_c + r0) fc) clamped to [0, nh) (get_HistIndex,
+// Codes_Folder/subrouts.cpp:795-812).  Counts per block in shared memory,
+// then one integer add per bin: the totals do not depend on the order.
+template <bool GEN>
+__global__ void __launch_bounds__(256) field_hist_kernel(const LatticeDev L, const double *__restrict__ state,
+                                                         const uint8_t *__restrict__ imp, int S, double r0,
+                                                         double fc, int nh, unsigned long long *hist)
+{
+    extern __shared__ unsigned int hs[];   // [nh][3]
+    for (int e = threadIdx.x; e < nh * 3; e += blockDim.x) hs[e] = 0u;
+    __syncthreads();
+    const int N = L.N;
+    const size_t total = (size_t)S * N;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const int s = (int)(e / N), i = (int)(e - (size_t)s * N);
+        const uint8_t *im = imp ? imp + (size_t)s * N : nullptr;
+        double h[3];
+        local_field<double, GEN>(L, state + (size_t)s * 3 * N, N, i, im ? im[i] : 0, im, h);
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            int k = (int)round((h[c] + r0) * fc);
+            k = k < 0 ? 0 : (k >= nh ? nh - 1 : k);
+            atomicAdd(&hs[k * 3 + c], 1u);
+        }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < nh * 3; e += blockDim.x)
+        if (hs[e]) atomicAdd(&hist[e], (unsigned long long)hs[e]);
+}
+
+cudaError_t launch_field_hist(const LatticeDev &L, const double *state, const uint8_t *imp, int S, double r0,
+                              double fc, int nh, unsigned long long *hist, bool gen, cudaStream_t st)
+{
+    const size_t total = (size_t)S * L.N;
+    const int blocks = (int)std::min<size_t>((total + 255) / 256, 148 * 8);
+    const size_t sm = (size_t)nh * 3 * sizeof(unsigned int);
+    if (gen) field_hist_kernel<true><<<blocks, 256, sm, st>>>(L, state, imp, S, r0, fc, nh, hist);
+    else field_hist_kernel<false><<<blocks, 256, sm, st>>>(L, state, imp, S, r0, fc, nh, hist);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_rk(const LatticeDev &L, const RKJob &J, int precision, bool gen,
                       cudaStream_t st)
 {

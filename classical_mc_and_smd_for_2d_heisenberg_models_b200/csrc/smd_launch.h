@@ -13,6 +13,15 @@ int rk_max_sites(int precision);
 cudaError_t launch_rk(const LatticeDev &L, const RKJob &J, int precision, bool gen,
                       cudaStream_t st);
 
+// local-field histograms of S samples ([S][3][N] FP64 state; imp [S][N] or
+// null): hist [nh][3] counts are added to (rk_kernels.cu)
+cudaError_t launch_field_hist(const LatticeDev &L, const double *state, const uint8_t *imp, int S, double r0,
+                              double fc, int nh, unsigned long long *hist, bool gen, cudaStream_t st);
+// static structure factor of S samples' grid transforms, series
+// [3][nqb][S] FP64, added to out [3][Q] in sample order (prepass.cu)
+cudaError_t launch_static_sf(const void *series, int Q, int nqb, int S, double cap, double *out,
+                             cudaStream_t st);
+
 // components per block of the grid transform (3 or 1); 0 when the grid
 // does not fit one block
 int grid_proj_ng(int G, int precision, const FFTPlan &p);

@@ -14,6 +14,11 @@
 //   outData/RK_Check/0WinTVec_<w>.dat, 0WinSpec_<w>.dat
 //                     the temporal window and its ordered spectrum
 //                     (smd_code.cpp:2808-2983)
+//   outData/RK_Results/MCSamples_DFT_{xy,yz,zz,tt}Spec<tag>.dat and
+//   outData/MC_Results/locFieldHist<tag>.dat
+//                     the static pre-pass over the samples: centred static
+//                     structure factor and local-field histograms
+//                     (smd_code.cpp:2289-2726), on the GPU
 //   outBin/MC_Bin_SpecData<tag>.bin
 //                     sample-averaged spectra, per q the ntm doubles of x,
 //                     y, z, then the autocorrelation (smd_code.cpp:3596-3631)
@@ -499,6 +504,46 @@ void record_2d(const Grid &g, const std::vector<double> &a, const std::string &p
     }
 }
 
+// C++ `fixed << showpos << setprecision(dg) << setw(wd)` (fmtDbleFix,
+// aux_code.cpp:530-541)
+std::string fix(double x, int dg, int wd)
+{
+    std::ostringstream o;
+    o << std::fixed << std::showpos << std::setprecision(dg) << std::setw(wd) << x;
+    return o.str();
+}
+
+// The static pre-pass records (smd_code.cpp:2641-2696): the centred static
+// structure factor MCSamples_DFT_{xy,yz,zz,tt}Spec and the local-field
+// histograms locFieldHist.  sf [3][G*G], hist [201][3] counts.
+void write_prepass(const Settings &s, const std::string &dir, const std::string &tag, int G,
+                   const std::vector<double> &sf, const std::vector<long long> &hist, double r0)
+{
+    const std::string res = dir + "/outData/RK_Results/", mcr = dir + "/outData/MC_Results/";
+    mkdirs(res);
+    mkdirs(mcr);
+    Grid g;
+    g.G = G;
+    g.c3 = s.c3();
+    g.dq = kPi2 / G;
+    const size_t Q = (size_t)G * G;
+    std::vector<double> a[4];
+    ordered(g, sf.data(), sf.data() + Q, sf.data() + 2 * Q, 1, 0, a);
+    const char *comp[4] = {"xy", "yz", "zz", "tt"};
+    for (int c = 0; c < 4; c++) record_2d(g, a[c], res + "MCSamples_DFT_" + comp[c] + "Spec" + tag + ".dat");
+    const int nh = 201;
+    const double box = 2.0 * r0 / (nh - 1);
+    double norm[3] = {0.0, 0.0, 0.0};
+    for (int k = 0; k < nh; k++)
+        for (int c = 0; c < 3; c++) norm[c] += (double)hist[(size_t)k * 3 + c];
+    std::ofstream f(mcr + "locFieldHist" + tag + ".dat");
+    for (int k = 0; k < nh; k++) {
+        f << fix(k * box - r0, 4, 8) << "  ";
+        for (int c = 0; c < 3; c++) f << fix((double)hist[(size_t)k * 3 + c] / norm[c], 4, 10) << "  ";
+        f << "\n";
+    }
+}
+
 // The text outputs of smd_code.cpp:3640-4130 from the sample-averaged
 // spectra spec [3][Q][ntm] and autocorrelation qss [ntm].
 void write_text(const Settings &s, const std::string &dir, const std::string &tag, int G, int ntm, double dtm_rec,
@@ -700,6 +745,16 @@ int main(int argc, char **argv)
             int lid = 0, qid = 0;
             check(smd_lattice_upload(ctx, &d, &lid), ctx, "smd_lattice_upload");
             check(smd_qset_upload(ctx, lid, 1, 0, nullptr, 1.0, &qid), ctx, "smd_qset_upload");
+            // the static pre-pass over every sample (smd_code.cpp:2289-2726)
+            {
+                std::vector<double> sf((size_t)3 * Q);
+                std::vector<long long> hist(201 * 3);
+                double r0 = 0.0;
+                check(smd_static_prepass(ctx, lid, qid, n, spins.data(), imp.empty() ? nullptr : imp.data(),
+                                         sf.data(), hist.data(), &r0),
+                      ctx, "smd_static_prepass");
+                write_prepass(s, dir, tag, G, sf, hist, r0);
+            }
             smd_job_desc j{};
             j.lattice = lid;
             j.qset = qid;

@@ -198,6 +198,24 @@ SMD_API int smd_dyn_spectrum_ref(smd_ctx *ctx, int lattice_id, int qset_id, doub
                          const int *imp, double *SqxWVec, double *SqyWVec,
                          double *SqzWVec, double *qSStVec);
 
+/* Static pre-pass over the MC samples (Codes_Folder/smd_code.cpp:2289-2726),
+ * the reference's first read of the sample file before any dynamics:
+ *   sf_out     [3][G*G] average over samples of the static structure factor
+ *              max(1e-16, |S_c(q)|^2) on the lattice's DFT grid, each
+ *              amplitude capped at spec0Max = 10, with the reference's
+ *              factor 1 / max(n_samples - 1, 1) (get_StaticSFac,
+ *              subrouts.cpp:8799-8825);
+ *   hist_out   [201][3] counts of the local-field components over every
+ *              site of every sample in 201 bins over +-max_field
+ *              (get_HistIndex, subrouts.cpp:795-812);
+ *   max_field  (out, may be NULL) maxLocField = sum over active shells of
+ *              max|J| times the shell's neighbours (subrouts.cpp:2081-2091).
+ * spins0 [n_samples][N][3] and imp [n_samples][N] (or NULL) on the host;
+ * qset_id must be a q set with the lattice's grid. */
+SMD_API int smd_static_prepass(smd_ctx *ctx, int lattice_id, int qset_id, int n_samples,
+                               const double *spins0, const int *imp, double *sf_out,
+                               long long *hist_out, double *max_field);
+
 /* RK evolution only (no projection): nsteps steps of the chosen form,
  * spins [n_samples][N][3] updated in place (host). */
 SMD_API int smd_evolve(smd_ctx *ctx, int lattice_id, int precision, int n_samples,

@@ -19,6 +19,10 @@
  *   sample loop     file read, checks, get_dynSpectrum, accumulation
  *                                             smd_code.cpp:3079-3291
  *
+ *   static pre-pass (--prepass) local-field histograms and the capped
+ *                   static structure factor of the samples, recorded as
+ *                   locFieldHist and MCSamples_DFT_*Spec
+ *                                                 smd_code.cpp:2289-2726
  *   output stage    (--outputs) sample averages, MC_Bin_SpecData, window
  *                   files, quantum-corrected zz spectra, centred slices, the
  *                   path and cut files            smd_code.cpp:2808-2983,
@@ -92,12 +96,13 @@ int main(int argc, char **argv)
     const string samples = argv[2];
     const long first = atol(argv[3]);
     const long count = atol(argv[4]);
-    bool dump_final = false, dwf_guard = true, outputs = false;
+    bool dump_final = false, dwf_guard = true, outputs = false, prepass = false;
     for (int a = 5; a < argc; a++) {
         string s = argv[a];
         if (s == "--dump-final") dump_final = true;
         if (s == "--no-dwf-guard") dwf_guard = false;
         if (s == "--outputs") outputs = true;
+        if (s == "--prepass") prepass = true;
     }
     if (chdir(workdir.c_str()) != 0) {
         cerr << "cannot enter " << workdir << "\n";
@@ -271,6 +276,72 @@ int main(int argc, char **argv)
     }
 
     double **spinField = Alloc_dble_array(Ns, 3);
+    if (prepass) {
+        /* The static pre-pass of smd_code.cpp:2289-2726 over samples
+           [first, first + count), calling the reference's functions. */
+        ostringstream oss0;
+        oss0 << fixed << setprecision(5) << Temp;
+        const string tTagDat = "_T(" + oss0.str() + ")" + outLabel + ".dat";
+        mkdir("outData", 0755);
+        mkdir("outData/MC_Results", 0755);
+        mkdir("outData/RK_Results", 0755);
+        const int NHist = 201;
+        const double hRange = 2.0 * maxLocField, boxSz = hRange / (NHist - 1), boxFc = 1.0 / boxSz;
+        complex<double> *Sqx = new complex<double>[Nq], *Sqy = new complex<double>[Nq];
+        complex<double> *Sqz = new complex<double>[Nq];
+        double **specField = Alloc_dble_array(Nq, 3), **CMT_spcFd = Alloc_dble_array(Nq, 3);
+        int **locFieldHist = Alloc_intg_array(NHist, 3);
+        init_dble_array(CMT_spcFd, Nq, 3, 0.0);
+        init_intg_array(locFieldHist, NHist, 3, 0);
+        Vec3d locField;
+        for (long s = first; s < first + count; s++) {
+            long pack = s / PackSize, in_pack = s % PackSize;
+            size_t base = pack * szCPack;
+            if (disOrder) {
+                fin.seekg(base, ios::beg);
+                fin.read(reinterpret_cast<char *>(impField), szIMap);
+                base += szIMap;
+            }
+            fin.seekg(base + in_pack * szConf, ios::beg);
+            for (int k = 0; k < Ns; k++) fin.read(reinterpret_cast<char *>(spinField[k]), 3 * sizeof(double));
+            for (int k = 0; k < Ns; k++) {
+                get_localField(k, spinField, locField);
+                locFieldHist[get_HistIndex(locField[0], maxLocField, boxFc, NHist)][0] += 1;
+                locFieldHist[get_HistIndex(locField[1], maxLocField, boxFc, NHist)][1] += 1;
+                locFieldHist[get_HistIndex(locField[2], maxLocField, boxFc, NHist)][2] += 1;
+            }
+            get_SqData_iMKL(spinField, Sqx, Sqy, Sqz);
+            for (int k = 0; k < Nq; k++) {
+                const double rx = abs(Sqx[k]), ry = abs(Sqy[k]), rz = abs(Sqz[k]);
+                Sqx[k] = min(spec0Max, rx) * Sqx[k] / rx;
+                Sqy[k] = min(spec0Max, ry) * Sqy[k] / ry;
+                Sqz[k] = min(spec0Max, rz) * Sqz[k] / rz;
+            }
+            get_StaticSFac(Sqx, Sqy, Sqz, specField);
+            for (int k = 0; k < Nq; k++)
+                for (int m = 0; m < 3; m++) CMT_spcFd[k][m] += specField[k][m];
+        }
+        const double fcs = 1.0 / max(count - 1, 1L);
+        for (int k = 0; k < Nq; k++)
+            for (int m = 0; m < 3; m++) specField[k][m] = fcs * CMT_spcFd[k][m];
+        double **xyA = Alloc_dble_array(Gsz, Gsz), **yzA = Alloc_dble_array(Gsz, Gsz);
+        double **zzA = Alloc_dble_array(Gsz, Gsz), **ttA = Alloc_dble_array(Gsz, Gsz);
+        dq = pi2 / Gsz;
+        get_OrderedSpecArray2D(specField, xyA, yzA, zzA, ttA);
+        record_SpecArray2D(xyA, "MCSamples_DFT_xySpec" + tTagDat, 1);
+        record_SpecArray2D(yzA, "MCSamples_DFT_yzSpec" + tTagDat, 1);
+        record_SpecArray2D(zzA, "MCSamples_DFT_zzSpec" + tTagDat, 1);
+        record_SpecArray2D(ttA, "MCSamples_DFT_ttSpec" + tTagDat, 1);
+        double histNorm[3] = {0.0, 0.0, 0.0};
+        for (int k = 0; k < NHist; k++)
+            for (int n = 0; n < 3; n++) histNorm[n] += locFieldHist[k][n];
+        ofstream recHist(outDir1 + subDir1 + "locFieldHist" + tTagDat);
+        for (int k = 0; k < NHist; k++) {
+            recHist << fmtDbleFix(k * boxSz - maxLocField, 4, 8) << X2;
+            for (int n = 0; n < 3; n++) recHist << fmtDbleFix(locFieldHist[k][n] / histNorm[n], 4, 10) << X2;
+            recHist << endl;
+        }
+    }
     double **SqxWVec = Alloc_dble_array(Nq, ntm);
     double **SqyWVec = Alloc_dble_array(Nq, ntm);
     double **SqzWVec = Alloc_dble_array(Nq, ntm);

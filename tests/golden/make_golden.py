@@ -99,7 +99,8 @@ def run_case(name, over, ntm, n, kind, sigma, seed, workroot):
 
 def run_text_case(name, over, ntm, n, kind, sigma, seed, workroot):
     """The reference's output stage on a spectrum case (smd_ref_run
-    --outputs): its MC_Bin_SpecData, window files, autocorrelation and every
+    --outputs --prepass): its static pre-pass records (MCSamples_DFT_*,
+    locFieldHist), MC_Bin_SpecData, window files, autocorrelation and every
     zz text file (slices, path, cut), stored as text_<name>.npz."""
     import subprocess
     s = SMDSettings(ntm=ntm, NMeas=1000 * max(n, 2), crSkip=1000, **over)
@@ -113,7 +114,7 @@ def run_text_case(name, over, ntm, n, kind, sigma, seed, workroot):
     path = os.path.join(wd, "samples.bin")
     smp.write_sample_file(path, s, spins, imp)
     r = subprocess.run([os.path.join(ROOT, "oracle", "_ref", "smd_ref_run"), wd, path, "0", str(n),
-                        "--no-dwf-guard", "--outputs"], capture_output=True, text=True)
+                        "--no-dwf-guard", "--outputs", "--prepass"], capture_output=True, text=True)
     if r.returncode:
         raise RuntimeError(r.stderr)
     files = {}
