@@ -211,17 +211,28 @@ def serving_leg(ctx, n_jobs: int, seed: int, fp64: bool = True):
            "job_shapes": [f"{w.settings.geom} N={w.settings.N} S={w.n_samples} "
                           f"steps={w.steps}" for w, *_ in prepared]}
     if fp64:
-        ms64, rels = 0.0, []
+        ms64, rels, floors = 0.0, [], []
         for (w, lid, qid, spins, imp_arr, win), (spec, _, _) in zip(prepared, burst):
-            r = ctx.run(lid, qid, spins, w.settings.dtm, w.n_rec, stride=w.stride,
-                        precision=_lib.SMD_FP64, fix_every=1, win=win, imp=imp_arr,
-                        want_final=False)
+            kw = dict(stride=w.stride, precision=_lib.SMD_FP64, fix_every=1, win=win,
+                      imp=imp_arr, want_final=False)
+            r = ctx.run(lid, qid, spins, w.settings.dtm, w.n_rec, **kw)
             ms64 += r.report["ms_device"]
             rels.append(rel_l2(spec, r.spec))
+            floor = None
+            if rels[-1] > 1e-3:
+                # a chaotic job: the FP64 form's own difference under one FP32
+                # rounding of its inputs
+                pert = workloads.tangent_perturb(spins, workloads.FP32_ROUNDOFF, 11)
+                floor = rel_l2(ctx.run(lid, qid, pert, w.settings.dtm, w.n_rec, **kw).spec, r.spec)
+            floors.append(floor)
         out["fp64_plain_site_steps_per_s"] = site_steps / (ms64 / 1e3)
         out["speedup_vs_fp64_plain"] = out["served_site_steps_per_s"] / out["fp64_plain_site_steps_per_s"]
-        out["dssf_rel_l2_vs_fp64"] = {"max": float(max(rels)), "median": float(np.median(rels)),
-                                      "per_job": [float(x) for x in rels]}
+        out["dssf_rel_l2_vs_fp64"] = {
+            "max": float(max(rels)), "median": float(np.median(rels)),
+            "per_job": [float(x) for x in rels],
+            "chaos_floor_per_job": floors,
+            "note": "chaos_floor: rel-L2 of the FP64 form from inputs moved by one FP32 rounding "
+                    "(2^-24) against the unperturbed FP64 run, taken for jobs above 1e-3"}
     return out
 
 
@@ -403,13 +414,29 @@ def run_ours(args, w, rank, world):
         if dist is not None:
             dist.all_reduce(t64, op=dist.ReduceOp.MAX)
         fp64_value = site_steps_rank * world * len(r64) / (float(t64.item()) / 1e3)
-        spec64 = d_spec.double().cpu().numpy()
+        spec64 = d_spec.double().cpu().numpy().copy()
+        # chaos floor: the FP64 form from inputs moved by one FP32 rounding
+        d_spins.copy_(torch.from_numpy(
+            workloads.tangent_perturb(spins, workloads.FP32_ROUNDOFF, 11)).to(d_spins.device))
+        device_step(_lib.SMD_FP64, 1)
+        spec64p = d_spec.double().cpu().numpy()
+        d_spins.copy_(torch.from_numpy(spins).to(d_spins.device))
         G2 = Q - (0 if ql is None else len(ql))   # grid q first, then the path
-        dssf = {"grid": rel_l2(spec32[:, :G2, :], spec64[:, :G2, :]),
-                "path": rel_l2(spec32[:, G2:, :], spec64[:, G2:, :]) if ql is not None else None,
-                "all": rel_l2(spec32, spec64),
-                "reference": "FP64 plain form (correction every step) on the same samples; "
-                             "that form equals the reference per spin to 1e-10 over 200 steps"}
+
+        def parts(a, b):
+            return {"grid": rel_l2(a[:, :G2, :], b[:, :G2, :]),
+                    "path": rel_l2(a[:, G2:, :], b[:, G2:, :]) if ql is not None else None,
+                    "all": rel_l2(a, b)}
+
+        dssf = parts(spec32, spec64)
+        dssf["chaos_floor"] = parts(spec64p, spec64)
+        dssf["reference"] = ("FP64 plain form (correction every step) on the same samples; that "
+                             "form equals the reference per spin to 1e-10 over 200 steps")
+        dssf["chaos_floor_note"] = (
+            "rel-L2 of the FP64 form run from the same samples moved by one FP32 rounding "
+            "(2^-24 tangent perturbation) against the unperturbed FP64 run: the trajectories "
+            "are chaotic over this length, so this is the least DSSF difference any FP32 "
+            "arithmetic can reach on this run")
         fp64 = {"value": fp64_value, "unit": UNIT,
                 "ms_per_step": float(t64.item()) / len(r64),
                 "ms_rk_per_step": sum(r.ms_rk for r in r64) / len(r64),

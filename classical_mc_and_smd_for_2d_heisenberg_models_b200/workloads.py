@@ -279,3 +279,21 @@ def make_inputs(w: Workload, rank: int = 0, lat=None):
         P = w.settings.pack_size
         imp_per_sample = np.stack([imp[k // P] for k in range(w.n_samples)])
     return spins, imp_per_sample
+
+
+# FP32 unit roundoff: the size of the rounding the FP32 form makes in every
+# stage, used as the input perturbation of the chaos-floor comparison
+FP32_ROUNDOFF = 2.0 ** -24
+
+
+def tangent_perturb(spins: np.ndarray, eps: float, seed: int) -> np.ndarray:
+    """Every spin moved by a seeded Gaussian tangent vector of rms size eps
+    and renormalised to |S| = 1.  Long SMD trajectories are chaotic: the
+    spectrum of an FP64 run from these inputs differs from the unperturbed
+    FP64 run by the least DSSF difference that any arithmetic making errors
+    of size eps can reach on that run (the chaos floor)."""
+    rng = np.random.default_rng(seed)
+    g = rng.normal(size=spins.shape) * eps
+    g -= (g * spins).sum(-1, keepdims=True) * spins
+    out = spins + g
+    return out / np.linalg.norm(out, axis=-1, keepdims=True)

@@ -369,27 +369,58 @@ def test_invalid_jobs_fail_loudly(ctx):
         ctx.run(lid, qid, spins, 0.01, 1)
 
 
-def test_fp32_form_at_c2_length(ctx):
-    """The benched workload's lattice and length -- triangular L = 48, 4096
-    records at stride 4 (16 380 RK steps, dt = 0.02), 48 x 48 grid plus the
-    512-point path -- on 4 of its samples: the FP32 form's spectrum is within
-    1e-3 (rel-L2, grid and path separately) of the FP64 form's, and its energy
-    drift stays within 1e-8 per site.  The FP64 form is the one pinned to the
-    reference per spin."""
+def _c2_forms(ctx, n_samples, n_rec):
+    """FP64, FP32 and FP32-roundoff-perturbed FP64 runs of the benched
+    workload's lattice (triangular L = 48, stride 4, dt = 0.02, 48 x 48 grid
+    plus the 512-point path) over n_rec records."""
     from classical_mc_and_smd_for_2d_heisenberg_models_b200 import workloads
-    w = workloads.c2(4)
+    w = workloads.c2(n_samples)
     s = w.settings
     lat, lid = _upload(ctx, s)
     ql = workloads.path_points(s.geom, w.qpath_points)
     qid = ctx.qset(lid, use_grid=True, qlist=ql)
     spins, _ = workloads.make_inputs(w)
-    win = smd.window(w.window, w.n_rec)
-    r64 = ctx.run(lid, qid, spins, s.dtm, w.n_rec, stride=w.stride, win=win, want_final=False)
-    r32 = ctx.run(lid, qid, spins, s.dtm, w.n_rec, stride=w.stride, win=win,
-                  precision=_lib.SMD_FP32, fix_every=w.fix_every, want_final=False)
+    win = smd.window(w.window, n_rec)
+    kw = dict(stride=w.stride, win=win, want_final=False)
+    r64 = ctx.run(lid, qid, spins, s.dtm, n_rec, **kw)
+    r32 = ctx.run(lid, qid, spins, s.dtm, n_rec, precision=_lib.SMD_FP32, fix_every=w.fix_every, **kw)
+    pert = workloads.tangent_perturb(spins, workloads.FP32_ROUNDOFF, 11)
+    r64p = ctx.run(lid, qid, pert, s.dtm, n_rec, **kw)
     G2 = lat.G * lat.G
-    for part in (slice(0, G2), slice(G2, None)):
-        a, b = r32.spec[:, part, :], r64.spec[:, part, :]
-        rel = np.linalg.norm(a - b) / np.linalg.norm(b)
-        assert rel <= 1e-3, (part, rel)
+    parts = {"grid": slice(0, G2), "path": slice(G2, None)}
+
+    def rel(a, b, part):
+        return np.linalg.norm(a.spec[:, part] - b.spec[:, part]) / np.linalg.norm(b.spec[:, part])
+
+    return r64, r32, r64p, parts, rel
+
+
+def test_fp32_form_within_1e3_before_the_chaotic_horizon(ctx):
+    """1024 records (4092 RK steps) of the benched workload on 4 samples,
+    a length over which an FP32-sized input perturbation has not yet grown
+    (the FP64 form's own sensitivity stays far below 1e-3): the FP32 form's
+    spectrum is within 1e-3 rel-L2 of the FP64 form's, grid and path
+    separately, with energy drift at most 1e-8 per site."""
+    r64, r32, r64p, parts, rel = _c2_forms(ctx, 4, 1024)
+    for name, part in parts.items():
+        assert rel(r64p, r64, part) <= 1e-4, (name, "the run is already chaotic")
+        assert rel(r32, r64, part) <= 1e-3, (name, rel(r32, r64, part))
+    assert r32.report["drift_max"] <= 1e-8 and r32.report["drift_final"] <= 1e-8, r32.report
+
+
+def test_fp32_form_at_c2_length_within_the_chaos_floor(ctx):
+    """The benched length -- 4096 records at stride 4, 16 380 RK steps -- on 8
+    samples.  Over this length the trajectories are chaotic: the FP64 form run
+    from inputs moved by one FP32 rounding (2^-24) ends with spins
+    decorrelated from the unperturbed run, and its spectrum differs by a few
+    1e-2.  No arithmetic that rounds at FP32 can get closer than that floor, so
+    the FP32 form's DSSF rel-L2 against the FP64 form must be of the floor's
+    order: at most 2 x the floor (grid and path separately; the FP32 form
+    rounds at every stage, not once at the start).  Its energy drift is at
+    most 1e-8 per site.  The FP64 form is the one pinned to the reference per
+    spin."""
+    r64, r32, r64p, parts, rel = _c2_forms(ctx, 8, 4096)
+    for name, part in parts.items():
+        floor = rel(r64p, r64, part)
+        assert rel(r32, r64, part) <= max(1e-3, 2.0 * floor), (name, rel(r32, r64, part), floor)
     assert r32.report["drift_max"] <= 1e-8 and r32.report["drift_final"] <= 1e-8, r32.report

@@ -36,7 +36,9 @@ def test_spec_binary_layout_round_trip(tmp_path):
 def test_driver_reproduces_reference_outputs(tmp_path, name):
     """Settings and sample files written in the reference's formats, the
     window as outBin/winvec.bin: the driver's MC_Bin_SpecData equals the
-    reference's sample average."""
+    reference's sample average.  The reference rescales a read window by
+    its maximum (Codes_Folder/smd_code.cpp:2828-2848), so the fixture's
+    spectrum, computed with the raw window, scales by 1 / max^2."""
     s, d = load_golden(name)
     n = int(d["n"])
     import dataclasses
@@ -53,7 +55,8 @@ def test_driver_reproduces_reference_outputs(tmp_path, name):
     rep = xsmd.run(wd, dwf_guard=False)
     Q = rep["Q"]
     spec, qss = xsmd.read_spec_bin(rep["spec_file"], Q, s.ntm)
-    ref = d["spec_sum"] / n
+    wmax = float(np.max(d["window"]))
+    ref = d["spec_sum"] / n / (wmax * wmax)
     assert np.max(np.abs(spec - ref)) <= 1e-10 * np.max(np.abs(ref))
     assert np.max(np.abs(qss - d["qss_sum"] / n)) <= 1e-10
     lines = open(rep["corr_file"]).read().splitlines()
