@@ -206,6 +206,23 @@ int member_ctas(Member &mb, int spt, int zt, size_t *smem)
     return 0;
 }
 
+// Clusters of a persistent RK launch: as many as fit the device at once
+// (maxc), less the clusters that would take the last `reserve` SMs.  The
+// projections of the previous chunk run on those SMs beside the RK launch,
+// as they do beside the single-job cluster kernel (whose samples leave SMs
+// free); without them the projections wait for the persistent launch to
+// drain.  SMD_RK_RESERVE_SMS sets the reserve (default 16 of 148).
+int rk_cluster_cap(int maxc, int csh)
+{
+    int dev = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm <= 0) nsm = 148;
+    const char *e = std::getenv("SMD_RK_RESERVE_SMS");
+    const int reserve = e ? std::max(0, std::atoi(e)) : 16;
+    const int cap = std::max(1, (nsm - reserve) / std::max(1, csh));
+    return std::min(maxc, cap);
+}
+
 // ------------------------------------------------------------ batches
 
 struct Config {
@@ -244,7 +261,7 @@ struct Batch {
 
 static_assert(sizeof(BatchParams) <= 32000, "batch parameters exceed the kernel-parameter limit");
 
-int zt_of(int z) { return z <= 8 ? 8 : z <= 12 ? 12 : z <= 18 ? 18 : -1; }
+int zt_of(int z) { return z <= 8 ? 8 : z <= 12 ? 12 : z <= 18 ? 18 : z <= 20 ? 20 : -1; }
 
 // Work items of one launch: (slot, first sample) for every member, CSH / CS
 // samples per item, members with the most sites per CTA first (their items
@@ -338,7 +355,7 @@ std::vector<Config> candidates(Batch &B)
             if (csh > kMaxClusterCTAs || csh < vmax || csh % vmax) continue;
             Config c = base;
             c.csh = csh;
-            c.nclusters = rk_batch_max_clusters(B.prec, spt, B.zt, c.threads, csh, c.smem);
+            c.nclusters = rk_cluster_cap(rk_batch_max_clusters(B.prec, spt, B.zt, c.threads, csh, c.smem), csh);
             if (c.nclusters > 0) out.push_back(c);
         }
     }

@@ -60,6 +60,9 @@ int launch_rk_members(smd_ctx *ctx, const std::vector<Member *> &m, const std::v
                       int zt, int spt, int threads, int csh, int nclusters, size_t smem, const int2 *d_items,
                       int n_items, int *d_queue, cudaStream_t st);
 int zt_of(int z);
+// Clusters of a persistent RK launch: at most maxc, leaving SMD_RK_RESERVE_SMS
+// SMs (default 16) to the projections that run beside it.
+int rk_cluster_cap(int maxc, int csh);
 
 // CTAs per sample of a member for a sites-per-thread value: the fewest (a
 // power of two) whose share of the sites fits a CTA of the batch kernel and

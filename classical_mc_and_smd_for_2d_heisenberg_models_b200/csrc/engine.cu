@@ -38,6 +38,7 @@
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <deque>
@@ -98,7 +99,9 @@ struct Engine {
     smd_ctx *parent = nullptr, *ectx = nullptr;
     cudaMemPool_t pool = nullptr;
     size_t budget = 0, used = 0;
-    int spt = 2, threads = 576;
+    // sites per thread of the batch kernel: 4 (512 threads) measured ahead of
+    // 2 on the serving mix, whose large lattices then take fewer CTAs per sample
+    int spt = 4, threads = 512;
     std::mutex mu;
     std::condition_variable cv, done_cv;
     std::deque<std::shared_ptr<SJob>> queue;
@@ -113,9 +116,14 @@ struct Engine {
     std::vector<int2> h_items[kSnapBufs][2];
     cudaEvent_t ev_rk[kSnapBufs]{}, ev_proj[kSnapBufs]{};
     std::map<long long, int> max_clusters;   // keyed by (prec, zt, csh, smem KiB)
+    // SMD_SERVE_TRACE=1: per-tick host and device times on stderr
+    bool trace = false;
+    cudaEvent_t tr[kSnapBufs][4]{};
+    Clock::time_point t_start = Clock::now();
 
     void run();
     int admit();
+    size_t room();
     int do_tick();
     void reap();
     void finish_job(SJob &j, int rc);
@@ -218,11 +226,28 @@ int Engine::run_alone(SJob &j)
     return rc;
 }
 
+// Device memory the pool can still hand out: free device memory plus what
+// the pool holds unused, less a margin for the context's own small
+// allocations.
+size_t Engine::room()
+{
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return budget;
+    cuuint64_t res = 0, inuse = 0;
+    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &res);
+    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &inuse);
+    const size_t avail = fr + (size_t)(res > inuse ? res - inuse : 0);
+    const size_t margin = (size_t)512 << 20;
+    return avail > margin ? avail - margin : 0;
+}
+
 // Admit sample groups of queued jobs, in arrival order, while slots and the
 // HBM budget allow.  Returns the number of groups admitted.
 int Engine::admit()
 {
     int admitted = 0;
+    bool halve_next = false;   // the last group's allocation failed: retry smaller
+    int last_S = 0;
     for (;;) {
         std::shared_ptr<SJob> jp;
         {
@@ -287,15 +312,21 @@ int Engine::admit()
             return m;
         };
         const int left = j.desc.n_samples - j.next_sample;
-        int S = left;
+        int S = halve_next ? std::max(1, last_S / 2) : left;
+        halve_next = false;
         std::unique_ptr<Member> m = make(S);
         size_t bytes = member_bytes(*m, m->Sp);
-        while (S > 1 && used + bytes > budget) {
+        // the group must fit the budget and the memory the device still has
+        // (other users of the device, this context's own buffers included)
+        const size_t free_now = room();
+        auto fits = [&](size_t b) { return used + b <= budget && b <= free_now; };
+        while (S > 1 && !fits(bytes)) {
             S = std::max(1, S / 2);
             m = make(S);
             bytes = member_bytes(*m, m->Sp);
         }
-        if (used + bytes > budget) {
+        last_S = S;
+        if (!fits(bytes)) {
             if (active.empty()) {
                 // not even one sample fits with nothing else resident
                 std::lock_guard<std::mutex> lk(mu);
@@ -329,7 +360,15 @@ int Engine::admit()
         DevBuf in;
         const size_t in_b = (size_t)S * m->N * 3 * 8;
         if (member_alloc(ectx, *m, pool, st) != SMD_OK || in.ensure_async(in_b, pool, st) != cudaSuccess) {
+            cudaGetLastError();   // the failed allocation's error is not sticky
+            m.reset();            // returns what was allocated to the pool
+            in.release();
             if (!active.empty()) return admitted;   // retry once memory is released
+            if (S > 1) {
+                // nothing else resident: retry with half the samples
+                halve_next = true;
+                continue;
+            }
             std::lock_guard<std::mutex> lk(mu);
             queue.pop_front();
             set_error("job " + std::to_string(j.id) + ": device allocation failed");
@@ -376,6 +415,21 @@ int Engine::do_tick()
         // projections of tick - 3 have read the snapshot buffers reused now
         CK(cudaEventSynchronize(ev_rk[bt]), "sync");
         CK(cudaStreamWaitEvent(srk, ev_proj[bt], 0), "wait");
+        if (trace) {
+            CK(cudaEventSynchronize(tr[bt][3]), "sync");
+            float a = 0.f, b = 0.f, c = 0.f;
+            cudaEventElapsedTime(&a, tr[bt][0], tr[bt][1]);
+            cudaEventElapsedTime(&b, tr[bt][2], tr[bt][3]);
+            cudaEventElapsedTime(&c, tr[bt][0], tr[bt][3]);
+            std::fprintf(stderr, "[smd serve] tick %lld: rk %.2f ms, projections %.2f ms, tick span %.2f ms\n",
+                         tick - kSnapBufs, a, b, c);
+        }
+    }
+    if (trace) {
+        std::fprintf(stderr, "[smd serve] tick %lld issued at %.1f ms: %zu groups, %.0f MB in use\n", tick,
+                     std::chrono::duration<double, std::milli>(Clock::now() - t_start).count(), active.size(),
+                     used / 1e6);
+        CK(cudaEventRecord(tr[bt][0], srk), "event");
     }
     CK(cudaMemsetAsync(d_queue[bt].p, 0, 2 * sizeof(int), srk), "memset");
     for (int prec : {SMD_FP32, SMD_FP64}) {
@@ -403,17 +457,20 @@ int Engine::do_tick()
         if (it == max_clusters.end())
             it = max_clusters.emplace(key, rk_batch_max_clusters(prec, spt, zt, threads, csh, smem)).first;
         if (it->second <= 0) return fail(ctx, SMD_ECUDA, "serving: no cluster of the RK launch fits the device");
+        const int ncl = rk_cluster_cap(it->second, csh);
         std::vector<int2> &hi = h_items[bt][prec];
         hi = make_items(mm, vcs, csh);
         CK(d_items[bt][prec].ensure(hi.size() * sizeof(int2)), "cudaMalloc");
         CK(cudaMemcpyAsync(d_items[bt][prec].p, hi.data(), hi.size() * sizeof(int2), cudaMemcpyHostToDevice, srk),
            "H2D items");
-        int rc = launch_rk_members(ctx, mm, chunk, prec, zt, spt, threads, csh, it->second, smem,
+        int rc = launch_rk_members(ctx, mm, chunk, prec, zt, spt, threads, csh, ncl, smem,
                                    d_items[bt][prec].as<int2>(), (int)hi.size(), d_queue[bt].as<int>() + prec, srk);
         if (rc) return rc;
     }
+    if (trace) CK(cudaEventRecord(tr[bt][1], srk), "event");
     CK(cudaEventRecord(ev_rk[bt], srk), "event");
     CK(cudaStreamWaitEvent(spr, ev_rk[bt], 0), "wait");
+    if (trace) CK(cudaEventRecord(tr[bt][2], spr), "event");
     int launches = 0;
     for (auto &g : active) {
         Member &m = *g.m;
@@ -431,6 +488,7 @@ int Engine::do_tick()
             CK(cudaMemcpyAsync(h, m.stats.p, (size_t)m.S * 32, cudaMemcpyDeviceToHost, spr), "D2H stats");
         }
     }
+    if (trace) CK(cudaEventRecord(tr[bt][3], spr), "event");
     CK(cudaEventRecord(ev_proj[bt], spr), "event");
     // finished groups leave; their buffers are released on the projection
     // stream, after the work that reads them
@@ -539,7 +597,10 @@ void Engine::run()
         }
     }
     budget = parent->budget;
-    if (const char *e = std::getenv("SMD_SERVE_SPT")) spt = std::atoi(e) == 4 ? 4 : 2;
+    if (const char *e = std::getenv("SMD_SERVE_TRACE")) trace = std::atoi(e) != 0;
+    for (int b = 0; b < kSnapBufs && trace; b++)
+        for (int k = 0; k < 4; k++) cudaEventCreate(&tr[b][k]);
+    if (const char *e = std::getenv("SMD_SERVE_SPT")) spt = std::atoi(e) == 2 ? 2 : 4;
     threads = rk_batch_threads(SMD_FP32, spt);
     for (;;) {
         {
@@ -591,6 +652,8 @@ void Engine::run()
         d_queue[b].release();
         if (ev_rk[b]) cudaEventDestroy(ev_rk[b]);
         if (ev_proj[b]) cudaEventDestroy(ev_proj[b]);
+        for (int k = 0; k < 4; k++)
+            if (tr[b][k]) cudaEventDestroy(tr[b][k]);
     }
     if (ectx) {
         cudaDeviceSynchronize();

@@ -250,7 +250,7 @@ extern "C" int smd_lattice_upload(smd_ctx *ctx, const smd_lattice_desc *d, int *
     if (!ctx || !d || !lattice_id) return SMD_EINVAL;
     if (d->N <= 0) return fail(ctx, SMD_EINVAL, "lattice: N must be positive");
     for (int s = 0; s < 3; s++) {
-        if (d->zn[s] < 0 || d->zn[s] > 6) return fail(ctx, SMD_EINVAL, "lattice: zn must lie in [0, 6]");
+        if (d->zn[s] < 0 || d->zn[s] > kMaxShellNb) return fail(ctx, SMD_EINVAL, "lattice: zn must lie in [0, 8]");
         if (d->shell_on[s] && d->zn[s] > 0 && !d->nbr[s])
             return fail(ctx, SMD_EINVAL, "lattice: missing neighbour table");
     }
@@ -497,7 +497,7 @@ ClusterTab *cluster_tables(Lattice &L, int CS, int zt_min)
     if (CS < 1 || CS > kMaxClusterCTAs || N < CS) return nullptr;
     const int zact = L.zn[0] + L.zn[1] + L.zn[2];
     const int zneed = std::max(zact, zt_min);
-    const int ZT = zneed <= 4 ? 4 : zneed <= 8 ? 8 : zneed <= 12 ? 12 : zneed <= 18 ? 18 : -1;
+    const int ZT = zneed <= 4 ? 4 : zneed <= 8 ? 8 : zneed <= 12 ? 12 : zneed <= 18 ? 18 : zneed <= 20 ? 20 : -1;
     if (ZT < 0) return nullptr;
     std::lock_guard<std::mutex> lk(L.cache_mu);
     auto it = L.ctabs.find({CS, ZT});

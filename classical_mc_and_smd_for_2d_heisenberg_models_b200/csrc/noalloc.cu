@@ -57,7 +57,7 @@ extern "C" int smd_evolve_fp64_noalloc(const smd_noalloc_model *m, int n_samples
     if (m->N <= 0 || n_samples <= 0 || nsteps < 1 || !(dt > 0.0)) return SMD_EINVAL;
     int ztot = 0;
     for (int s = 0; s < 3; s++) {
-        if (m->zn[s] < 0 || m->zn[s] > 6) return SMD_EINVAL;
+        if (m->zn[s] < 0 || m->zn[s] > kMaxShellNb) return SMD_EINVAL;
         ztot += m->zn[s];
     }
     if (ztot == 0 || m->N > rk_max_sites(SMD_FP64)) return SMD_EINVAL;

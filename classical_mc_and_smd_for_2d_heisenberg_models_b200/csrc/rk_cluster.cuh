@@ -24,7 +24,7 @@
 
 namespace smd {
 
-constexpr int kMaxEdgeSlots = 18;
+constexpr int kMaxEdgeSlots = 20;
 constexpr int kMaxClusterCTAs = 16;
 
 struct ClusterParams {

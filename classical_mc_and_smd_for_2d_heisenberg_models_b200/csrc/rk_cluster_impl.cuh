@@ -838,6 +838,7 @@ cudaError_t launch_batch_spt(const BatchParams *B, int zt, int threads, int csh,
     case 8: return launch_batch_t<T, SPT, 8>(B, threads, csh, nclusters, smem, st, max_clusters);
     case 12: return launch_batch_t<T, SPT, 12>(B, threads, csh, nclusters, smem, st, max_clusters);
     case 18: return launch_batch_t<T, SPT, 18>(B, threads, csh, nclusters, smem, st, max_clusters);
+    case 20: return launch_batch_t<T, SPT, 20>(B, threads, csh, nclusters, smem, st, max_clusters);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -888,6 +889,7 @@ cudaError_t launch_cluster_spt(const ClusterParams &P, const RKJob &J, int threa
     case 8: return launch_cluster_t<T, SPT, 8>(P, J, threads, smem, st);
     case 12: return launch_cluster_t<T, SPT, 12>(P, J, threads, smem, st);
     case 18: return launch_cluster_t<T, SPT, 18>(P, J, threads, smem, st);
+    case 20: return launch_cluster_t<T, SPT, 20>(P, J, threads, smem, st);
     default: return cudaErrorInvalidValue;
     }
 }

@@ -66,7 +66,7 @@ __device__ __forceinline__ void local_field(const LatticeDev &L, const T *__rest
         const int zs = L.zn[s];
         const int *nb = L.nbr + (size_t)L.zoff[s] * N + i;
 #pragma unroll
-        for (int k = 0; k < 6; k++) {
+        for (int k = 0; k < kMaxShellNb; k++) {
             if (k < zs) {
                 const int j = __ldg(nb + (size_t)k * N);
                 if (j >= 0) {
@@ -119,7 +119,7 @@ __device__ __forceinline__ void local_field_lower(const LatticeDev &L, const dou
         const int zs = L.zn[s];
         const int *nb = L.nbr + (size_t)L.zoff[s] * N + i;
 #pragma unroll
-        for (int k = 0; k < 6; k++) {
+        for (int k = 0; k < kMaxShellNb; k++) {
             if (k < zs) {
                 const int j = __ldg(nb + (size_t)k * N);
                 if (j >= 0) {

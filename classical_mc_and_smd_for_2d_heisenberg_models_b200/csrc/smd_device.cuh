@@ -19,6 +19,11 @@
 
 namespace smd {
 
+// Most neighbours of one shell: 6 on the crystal lattices, 8 on the
+// Ammann-Beenker approximants (Zn1 = ZnX = 8, Zn2 = 3;
+// Codes_Folder/subrouts.cpp:1006-1012).
+constexpr int kMaxShellNb = 8;
+
 struct LatticeDev {
     int N;
     int zn[3];

@@ -71,6 +71,14 @@ def ordered_state(s: SMDSettings, kind: str) -> np.ndarray:
     ``ferro``:  S = z.
     Sites are numbered k = i * L + j (Codes_Folder/subrouts.cpp:2700-2708).
     """
+    if s.qcrystal:
+        # a quasi-crystal has no Bravais cell: only the uniform state here
+        # (its ordered states come as table files, see smd.load_qcrystal)
+        if kind != "ferro":
+            raise ValueError(f"{kind}: pass the approximant's state file as base")
+        S = np.zeros((s.N, 3))
+        S[:, 2] = 1.0
+        return S
     L = s.L
     i, j = np.meshgrid(np.arange(L), np.arange(L), indexing="ij")
     i = i.ravel().astype(np.float64)

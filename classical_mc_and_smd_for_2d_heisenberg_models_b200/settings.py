@@ -39,6 +39,12 @@ GEOMETRY = {
     "lieb": (2, 2, (4, 4, 4)),
 }
 
+# quasi-crystal approximants read from table files (qcrystal = 1):
+# Ammann-Beenker tilings, Codes_Folder/subrouts.cpp:1006-1012
+QCT_GEOMETRY = {
+    "Aamman": (1, 1, (8, 3, 8)),
+}
+
 BIN_SZ = 1000          # Codes_Folder/subrouts.cpp:309
 TEMP_MAX = 2.0         # Codes_Folder/subrouts.cpp:389
 DWF_MIN = 0.10         # Codes_Folder/subrouts.cpp:391
@@ -98,24 +104,51 @@ class SMDSettings:
 
     # ------------------------------------------------------------ derived
     @property
+    def qcrystal(self) -> bool:
+        """A lattice read from table files; L then holds the site count
+        (the reference's latSize, Codes_Folder/subrouts.cpp:1105-1114)."""
+        return bool(self.flags.get("qcrystal", 0))
+
+    def _geo(self):
+        table = QCT_GEOMETRY if self.qcrystal else GEOMETRY
+        if self.geom not in table:
+            raise SettingsError(f"unknown geometry {self.geom!r}")
+        return table[self.geom]
+
+    @property
     def nsubs(self) -> int:
-        return GEOMETRY[self.geom][0]
+        return self._geo()[0]
 
     @property
     def grid_fac(self) -> int:
-        return GEOMETRY[self.geom][1]
+        return self._geo()[1]
 
     @property
     def zn(self):
-        return GEOMETRY[self.geom][2]
+        return self._geo()[2]
 
     @property
     def N(self) -> int:
+        if self.qcrystal:
+            return self.L
         return self.nsubs * self.L * self.L
 
     @property
+    def Lsz(self) -> int:
+        """Lattice length; for a quasi-crystal the even integer below
+        sqrt(N), the side of its square q set (subrouts.cpp:1111)."""
+        if self.qcrystal:
+            return (int(math.sqrt(self.L)) // 2) * 2
+        return self.L
+
+    @property
     def G(self) -> int:
-        return self.grid_fac * self.L
+        return self.grid_fac * self.Lsz
+
+    @property
+    def size_tag(self) -> str:
+        """SzTag of the table and sample file names (subrouts.cpp:1109)."""
+        return f"_AppxtSz({self.L})" if self.qcrystal else ""
 
     @property
     def disorder(self) -> bool:
@@ -178,12 +211,19 @@ class SMDSettings:
     # ----------------------------------------------------------- checks
     def validate(self, check_dwf: bool = True) -> None:
         """The input checks of convert_inputs2data and main that apply to SMD."""
-        if self.geom not in GEOMETRY:
-            raise SettingsError(f"unknown geometry {self.geom!r}")
-        if self.L % 2:
-            raise SettingsError("lattice length must be a multiple of 2")
-        if self.geom not in ("square", "lieb") and self.L % 3:
-            raise SettingsError("lattice length must be a multiple of 3")
+        self._geo()
+        if self.qcrystal:
+            # smd_code.cpp:365-372: a quasi-crystal run needs PBC_OFF = 1 and
+            # qct_RemovePBC = 0
+            if self.flags.get("qct_RemovePBC", 0) or not self.flags.get("PBC_OFF", 0):
+                raise SettingsError("qcrystal needs PBC_OFF = 1 and qct_RemovePBC = 0")
+            if self.L < 4:
+                raise SettingsError("quasi-crystal size too small")
+        else:
+            if self.L % 2:
+                raise SettingsError("lattice length must be a multiple of 2")
+            if self.geom not in ("square", "lieb") and self.L % 3:
+                raise SettingsError("lattice length must be a multiple of 3")
         if _is_not_zero(self.J2_delta) and self.geom != "lieb":
             raise SettingsError("J2_delta requires the lieb geometry")
         if self.NMeas % BIN_SZ or self.NMeas // BIN_SZ == 1:

@@ -49,6 +49,10 @@ class Lattice:
     def grid_fac(self) -> int:
         return self.G // self.L
 
+    @property
+    def qcrystal(self) -> bool:
+        return self.grid_map is None
+
     def grid_positions(self) -> np.ndarray:
         """Site positions in the frame of the DFT grid.
 
@@ -57,8 +61,11 @@ class Lattice:
         indices (a, b); the grid is the lattice shifted by i0 cells along x
         for lieb and kagome (Codes_Folder/subrouts.cpp:2905-2936).  Positions
         R = a fc e1 + b fc e2 make exp(-i q . R) equal those phases at grid
-        q, so list points reproduce grid values exactly.
+        q, so list points reproduce grid values exactly.  A quasi-crystal's
+        positions are its table's (rvecList).
         """
+        if self.qcrystal:
+            return self.rvec.copy()
         sz = {"square": 1.0, "triang": 1.0, "hexagn": math.sqrt(3.0), "kagome": 2.0,
               "lieb": math.sqrt(2.0)}[self.geom]
         fc = sz / self.grid_fac
@@ -109,6 +116,60 @@ def build_lattice(geom: str, L: int) -> Lattice:
     if rc:
         raise SMDError(rc, f"smd_build_lattice({geom}, {L})")
     return Lattice(geom, L, N, G, ns, zn, rvec, gmap, nb)
+
+
+def load_qcrystal(table_dir: str, N: int, geom: str = "Aamman") -> Lattice:
+    """A quasi-crystal approximant from the reference's table files in
+    ``table_dir`` (the outBin/ folder of a qcrystal run):
+
+      sitesList_AppxtSz(N).bin  N x 2 doubles, the site positions (rvecList)
+      nborsList_AppxtSz(N).bin  per site Zn1, Zn2 then ZnX int32 neighbour
+                                indices, -1 where a site has fewer (ghosts)
+
+    as Codes_Folder/smd_code.cpp:1248-1300 and 1575-1660 read them, with
+    the same checks: exact file sizes and a unit nearest-neighbour spacing
+    (check_latticeSpc, Codes_Folder/subrouts.cpp:5803-5832).  The returned
+    lattice has no DFT grid (G = the side of its direct-sum q set)."""
+    import os
+    from .settings import QCT_GEOMETRY, SettingsError
+    if geom not in QCT_GEOMETRY:
+        raise SettingsError(f"unknown quasi-geometry {geom!r}")
+    zn = list(QCT_GEOMETRY[geom][2])
+    tag = f"_AppxtSz({N})"
+    sites = os.path.join(table_dir, f"sitesList{tag}.bin")
+    nbors = os.path.join(table_dir, f"nborsList{tag}.bin")
+    if not os.path.exists(sites) or os.path.getsize(sites) != N * 16:
+        raise SettingsError(f"invalid or missing {sites}")
+    if not os.path.exists(nbors) or os.path.getsize(nbors) != N * sum(zn) * 4:
+        raise SettingsError(f"invalid or missing {nbors}")
+    rvec = np.fromfile(sites, dtype=np.float64).reshape(N, 2)
+    tab = np.fromfile(nbors, dtype=np.int32).reshape(N, sum(zn))
+    if tab.max() >= N:
+        raise SettingsError(f"{nbors}: neighbour index out of range")
+    nb = [np.ascontiguousarray(tab[:, :zn[0]]),
+          np.ascontiguousarray(tab[:, zn[0]:zn[0] + zn[1]]),
+          np.ascontiguousarray(tab[:, zn[0] + zn[1]:])]
+    # check_latticeSpc: shortest first-shell distance from site 0 (entries
+    # > 0, as the reference tests them) within 5 % of one
+    d = [float(np.hypot(*(rvec[j] - rvec[0]))) for j in nb[0][0] if j > 0]
+    if not d or not (0.95 <= min(d) <= 1.05):
+        raise SettingsError("lattice spacing is not unit")
+    Lsz = (int(math.sqrt(N)) // 2) * 2
+    return Lattice(geom, Lsz, N, Lsz, 1, zn, rvec, None, nb)
+
+
+def qcrystal_qpoints(lat: Lattice) -> Tuple[np.ndarray, float]:
+    """The q set and scale of get_qct_SqData (Codes_Folder/subrouts.cpp:
+    8460-8525) for a quasi-crystal: Lsz x Lsz points q = dq (nx, ny), nx
+    and ny in FFT order (0 .. Lsz/2 - 1, then -Lsz/2 .. -1), output index
+    j Lsz + i for (nx(i), ny(j)), dq = 4 (2 pi) / Lsz
+    (Codes_Folder/smd_code.cpp:1774), scale 1 / sqrt(N)."""
+    L = lat.G
+    dq = 4.0 * (2.0 * math.pi) / L
+    n = np.where(np.arange(L) < L // 2, np.arange(L), np.arange(L) - L)
+    ny, nx = np.meshgrid(n, n, indexing="ij")     # row j (ny), column i (nx)
+    q = np.stack([nx.ravel() * dq, ny.ravel() * dq], axis=1)
+    return q, 1.0 / math.sqrt(lat.N)
 
 
 def build_bonds(lat: Lattice, j2_on: bool, jx_on: bool):
@@ -176,7 +237,7 @@ class Context:
         """Upload a lattice with the couplings of settings ``s``."""
         bonds, nbonds = build_bonds(lat, s.j2_on, s.jx_on)
         nb = [np.ascontiguousarray(a, np.int32) for a in lat.nbrs]
-        gmap = np.ascontiguousarray(lat.grid_map, np.int32)
+        gmap = None if lat.qcrystal else np.ascontiguousarray(lat.grid_map, np.int32)
         pos = np.ascontiguousarray(lat.grid_positions(), np.float64)
         d = _lib.LatticeDesc()
         d.N = lat.N
@@ -199,8 +260,9 @@ class Context:
         for k in range(3):
             d.nbonds[k] = nbonds[k]
         d.bonds = bonds.ctypes.data
-        d.G = lat.G
-        d.grid_map = gmap.ctypes.data
+        # a quasi-crystal has no DFT grid: its q set is a direct-sum list
+        d.G = 0 if lat.qcrystal else lat.G
+        d.grid_map = None if gmap is None else gmap.ctypes.data
         d.pos = pos.ctypes.data
         lid = C.c_int()
         self._check(self.lib.smd_lattice_upload(self.h, C.byref(d), C.byref(lid)), "lattice upload")

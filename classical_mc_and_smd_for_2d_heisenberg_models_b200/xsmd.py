@@ -108,11 +108,19 @@ def run(workdir: str, device: int = 0, precision=None, stride=None, fix_every=No
     tag = s.t_tag
     spins, imp = smp.read_sample_file(os.path.join(workdir, "outBin", smp.sample_file_name(s)), s)
     win = _window(s, workdir)
-    lat = smd.build_lattice(s.geom, s.L)
+    if s.qcrystal:
+        # tables from outBin/ and the direct-sum q set of get_qct_SqData
+        lat = smd.load_qcrystal(os.path.join(workdir, "outBin"), s.N, s.geom)
+    else:
+        lat = smd.build_lattice(s.geom, s.L)
     t0 = time.perf_counter()
     with smd.Context(device) as ctx:
         lid = ctx.lattice(s, lat)
-        qid = ctx.qset(lid, use_grid=True)
+        if s.qcrystal:
+            q, sc = smd.qcrystal_qpoints(lat)
+            qid = ctx.qset(lid, use_grid=False, qlist=q, list_scale=sc)
+        else:
+            qid = ctx.qset(lid, use_grid=True)
         prec = _lib.SMD_FP64 if o["precision"] == "fp64" else _lib.SMD_FP32
         # ntm records: ntm - 1 steps at stride 1, as the reference records
         # every step (subrouts.cpp:11734)

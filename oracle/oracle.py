@@ -98,6 +98,32 @@ def make_lattice(geom: str, L: int) -> Dict:
                 grid_map=gmap, nbrs=nb)
 
 
+def tables_lattice(rvec: np.ndarray, nbrs, G: int) -> Dict:
+    """A lattice given by its tables (a quasi-crystal approximant read from
+    the reference's sitesList / nborsList files, smd_code.cpp:1248-1300 and
+    1575-1660): positions, three neighbour tables with -1 ghosts, no DFT
+    grid (grid_map all -1), G the side of the direct-sum q set."""
+    nb = [np.ascontiguousarray(a, np.int32) for a in nbrs]
+    N = len(rvec)
+    return dict(geom="table", L=G, N=N, G=G, nsubs=1, zn=[a.shape[1] for a in nb],
+                rvec=np.ascontiguousarray(rvec, np.float64),
+                grid_map=np.full(G * G, -1, np.int32), nbrs=nb)
+
+
+def qct_qpoints(G: int, N: int):
+    """q set of get_qct_SqData (Codes_Folder/subrouts.cpp:8460-8525): for
+    output index j G + i, q = dq (nx(i), ny(j)) with n(i) = i for i < G/2,
+    else i - G, and dq = 4 pi2 / G (smd_code.cpp:1774); scale 1/sqrt(N)."""
+    dq = 4.0 * (2.0 * np.pi) / G
+    q = np.zeros((G * G, 2))
+    for j in range(G):
+        ny = j if j < G // 2 else j - G
+        for i in range(G):
+            nx = i if i < G // 2 else i - G
+            q[j * G + i] = (nx * dq, ny * dq)
+    return q, 1.0 / np.sqrt(N)
+
+
 def make_bonds(lat: Dict, j2_on: bool, jx_on: bool):
     N, zn = lat["N"], lat["zn"]
     maxb = N * sum(zn)

@@ -129,8 +129,10 @@ int main(int argc, char **argv)
         qct_NeelPhase = vals[13]; qct_RemovePBC = vals[14];
         rec_orderMaps = vals[15];
     }
-    if (qcrystal || FFTW_ON || !with_DFTcodes) {
-        cerr << "runner supports periodic crystals with with_DFTcodes=1\n";
+    if (qcrystal ? (qct_RemovePBC || !PBC_OFF) : (FFTW_ON || !with_DFTcodes)) {
+        /* quasi-crystals: the reference's own check (smd_code.cpp:365-372) */
+        cerr << "runner supports periodic crystals with with_DFTcodes=1, or"
+                " quasi-crystals with PBC_OFF=1 and qct_RemovePBC=0\n";
         return 3;
     }
 
@@ -155,22 +157,49 @@ int main(int argc, char **argv)
 
     /* ---- lattice */
     rvecList = Alloc_dble_array(Ns, 2);
-    if (multiSubs) r0List = Alloc_dble_array(Ns0, 2);
-    dftGrid = Alloc_dble_array(Nsg, 2);
-    gridMap = new int[Nsg];
-    make_rvecList(flag);
-    if (flag > 0) {
-        cerr << "make_rvecList failed " << flag << "\n";
-        return 5;
-    }
     nbors1 = Alloc_intg_array(Ns, Zn1);
     nbors2 = Alloc_intg_array(Ns, Zn2);
     nborsX = Alloc_intg_array(Ns, ZnX);
-    mkdir("outBin", 0755);
-    make_nborsTable(flag);
-    if (flag > 0) {
-        cerr << "make_nborsTable failed " << flag << "\n";
-        return 5;
+    if (qcrystal) {
+        /* tables read from outBin/ as smd_code.cpp:1248-1300 (sites) and
+           1575-1660 (neighbours) read them, with their size checks and the
+           reference's lattice-spacing check */
+        ifstream st(outDir0 + "sitesList" + SzTag + ".bin", ios::binary | ios::ate);
+        ifstream nb(outDir0 + "nborsList" + SzTag + ".bin", ios::binary | ios::ate);
+        if (!st.is_open() || !nb.is_open() || (size_t)st.tellg() != (size_t)Ns * 2 * sizeof(double) ||
+            (size_t)nb.tellg() != (size_t)Ns * (Zn1 + Zn2 + ZnX) * sizeof(int)) {
+            cerr << "missing or invalid quasi-crystal tables\n";
+            return 5;
+        }
+        st.seekg(0, ios::beg);
+        nb.seekg(0, ios::beg);
+        for (int k = 0; k < Ns; k++) st.read(reinterpret_cast<char *>(rvecList[k]), 2 * sizeof(double));
+        for (int k = 0; k < Ns; k++) {
+            nb.read(reinterpret_cast<char *>(nbors1[k]), Zn1 * sizeof(int));
+            nb.read(reinterpret_cast<char *>(nbors2[k]), Zn2 * sizeof(int));
+            nb.read(reinterpret_cast<char *>(nborsX[k]), ZnX * sizeof(int));
+        }
+        double lspc = 0.0;
+        check_latticeSpc(lspc, flag);
+        if (flag > 0) {
+            cerr << "lattice spacing is not unit\n";
+            return 5;
+        }
+    } else {
+        if (multiSubs) r0List = Alloc_dble_array(Ns0, 2);
+        dftGrid = Alloc_dble_array(Nsg, 2);
+        gridMap = new int[Nsg];
+        make_rvecList(flag);
+        if (flag > 0) {
+            cerr << "make_rvecList failed " << flag << "\n";
+            return 5;
+        }
+        mkdir("outBin", 0755);
+        make_nborsTable(flag);
+        if (flag > 0) {
+            cerr << "make_nborsTable failed " << flag << "\n";
+            return 5;
+        }
     }
     {
         int nbonds[4];
@@ -193,7 +222,12 @@ int main(int argc, char **argv)
         for (int k = 0; k < Ns; k++) put(f, nbors1[k], Zn1);
         for (int k = 0; k < Ns; k++) put(f, nbors2[k], Zn2);
         for (int k = 0; k < Ns; k++) put(f, nborsX[k], ZnX);
-        put(f, gridMap, (size_t)Nsg);
+        if (qcrystal) {
+            vector<int> none((size_t)Nsg, -1);   /* no DFT grid */
+            put(f, none.data(), none.size());
+        } else {
+            put(f, gridMap, (size_t)Nsg);
+        }
         for (int k = 0; k < Nb; k++) {
             int b[2] = {bondList[k].x, bondList[k].y};
             put(f, b, 2);
@@ -208,11 +242,16 @@ int main(int argc, char **argv)
         cerr << "dwf " << dwf << " exceeds dwf_min\n";
         return 6;
     }
-    {
+    if (!qcrystal) {
         MKL_LONG dims[2] = {Gsz, Gsz};
         DftiCreateDescriptor(&handle, DFTI_DOUBLE, DFTI_COMPLEX, 2, dims);
         DftiCommitDescriptor(handle);
+    } else if (prepass || outputs) {
+        cerr << "--prepass and --outputs need a periodic crystal\n";
+        return 3;
     }
+    /* the direct-sum q spacing of a quasi-crystal (smd_code.cpp:1774) */
+    if (qcrystal) dq = 4.0 * pi2 / Gsz;
 
     /* ---- temporal window */
     double *tmWinVec = new double[ntm];

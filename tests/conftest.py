@@ -24,6 +24,14 @@ def load_golden(name):
     return s, d
 
 
+def golden_lattice(oracle_mod, s, d):
+    """The oracle's lattice of a fixture: built from the geometry for a
+    crystal, from the fixture's reference tables for a quasi-crystal."""
+    if s.qcrystal:
+        return oracle_mod.tables_lattice(d["rvec"], (d["nb1"], d["nb2"], d["nbx"]), s.G)
+    return oracle_mod.make_lattice(s.geom, s.L)
+
+
 def golden_names(prefix=""):
     """Fixture names with the prefix; without one, the trajectory and
     spectrum cases (the text_ output-stage fixtures have another layout)."""

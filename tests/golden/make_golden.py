@@ -16,7 +16,7 @@ Spectrum cases also get text_<name>.npz: the reference's output stage
 files, autocorrelation) through smd_ref_run --outputs.
 
 Run from the repository root (needs the reference sources at build time):
-    make -C oracle ref && python tests/golden/make_golden.py [--text]
+    make -C oracle ref && python tests/golden/make_golden.py [--text | --qct]
 """
 from __future__ import annotations
 
@@ -61,6 +61,60 @@ CASES = [
     ("spec_lieb_disorder", dict(geom="lieb", L=4, J2=0.4, imp_ratio=0.1, J1ic=0.5, J2ic=0.2,
                                 J1ii=0.3, dtm=0.02, window="ntall"), 16, 2, "ferro", 0.7, 25),
 ]
+
+
+# Quasi-crystal cases (qcrystal = 1): the reference's Ammann-Beenker
+# approximant tables from QCrystal_Data/ copied into the work directory's
+# outBin/, samples tilted from one of the approximant's ordered states.
+# (name, table folder, N, settings overrides, ntm, samples, state, sigma, seed)
+QCT_DIR = "/root/reference/QCrystal_Data"
+QCT_CASES = [
+    ("traj_qct239_pbc", "with_PBC/239", 239, dict(J2=0.3, dtm=0.01), 201, 2, "stateNeel0", 0.2, 31),
+    ("traj_qct239_open_xxz_h", "no_PBC/239", 239, dict(J2=0.25, JX=0.1, zlamb1=0.9, zlamb2=0.9,
+                                                        h=0.2, dtm=0.01), 201, 1, "stateStrp2", 0.2, 33),
+    ("spec_qct239_open", "no_PBC/239", 239, dict(J2=0.2, JX=0.1, dtm=0.02, window="hann1"), 16, 2,
+     "stateStrp1", 0.3, 32),
+    # more sites than one CTA holds: the lattice is split over a cluster
+    ("traj_qct1393_pbc_jx", "with_PBC/1393", 1393, dict(J2=0.3, JX=0.1, dtm=0.01), 101, 1,
+     "stateStrp3", 0.2, 34),
+]
+
+
+def run_qct_case(name, folder, N, over, ntm, n, state, sigma, seed, workroot):
+    import shutil
+    s = SMDSettings(geom="Aamman", L=N, ntm=ntm, NMeas=1000 * max(n, 2), crSkip=1000, **over)
+    s.flags["qcrystal"] = 1
+    s.flags["PBC_OFF"] = 1
+    s.validate(check_dwf=False)
+    wd = os.path.join(workroot, name)
+    s.write(wd)
+    os.makedirs(os.path.join(wd, "outBin"), exist_ok=True)
+    src = os.path.join(QCT_DIR, folder)
+    tag = s.size_tag
+    for f in (f"sitesList{tag}.bin", f"nborsList{tag}.bin"):
+        shutil.copy(os.path.join(src, f), os.path.join(wd, "outBin", f))
+    base = np.fromfile(os.path.join(src, f"{state}{tag}.bin")).reshape(N, 3)
+    total = max(n, 2)
+    spins, _ = smp.make_samples(s, total, "ferro", sigma, seed, base=base)
+    path = os.path.join(wd, "samples.bin")
+    smp.write_sample_file(path, s, spins, None)
+    info = O.run_reference(wd, path, 0, n, dump_final=True, dwf_guard=False)
+    lat = O.read_ref_lattice(wd)
+    spec, qss = O.read_ref_spec(wd, s.G * s.G, ntm)
+    final = O.read_ref_final(wd, n, s.N)
+    win = O.window(s.window, ntm) if s.window != "nowin" else np.ones(ntm)
+    out = dict(
+        settings=json.dumps(dataclasses.asdict(s)),
+        spins0=spins[:n], final=final, spec_sum=spec, qss_sum=qss,
+        rvec=lat["rvec"], grid_map=lat["grid_map"], nb1=lat["nbrs"][0], nb2=lat["nbrs"][1],
+        nbx=lat["nbrs"][2], bonds=lat["bonds"], nbonds=np.array(lat["nbonds"], np.int32),
+        window=win, n=np.int32(n), qct_table=np.array(folder),
+    )
+    if name.startswith("traj_"):
+        out.pop("spec_sum")
+        out.pop("qss_sum")
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+    return info
 
 
 def run_case(name, over, ntm, n, kind, sigma, seed, workroot):
@@ -136,7 +190,13 @@ def main():
     if not O.reference_available():
         raise SystemExit("oracle/_ref/smd_ref_run is missing: run `make -C oracle ref` first")
     text_only = "--text" in sys.argv
+    qct_only = "--qct" in sys.argv
     with tempfile.TemporaryDirectory() as tmp:
+        if not text_only:
+            for c in QCT_CASES:
+                print(c[0], run_qct_case(*c, tmp))
+        if qct_only:
+            return
         for c in CASES:
             if not text_only:
                 info = run_case(*c, tmp)

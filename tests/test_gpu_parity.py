@@ -21,15 +21,30 @@ SPIN_TOL = 1e-10
 SPEC_TOL = 1e-10
 
 
-def _upload(ctx, s):
-    lat = smd.build_lattice(s.geom, s.L)
+def _upload(ctx, s, d=None):
+    """Build and upload a lattice: from the geometry for a crystal, from the
+    fixture's reference tables (sitesList / nborsList) for a quasi-crystal."""
+    if s.qcrystal:
+        lat = smd.Lattice(s.geom, s.G, s.N, s.G, 1, list(s.zn), np.asarray(d["rvec"]), None,
+                          [np.asarray(d[k]) for k in ("nb1", "nb2", "nbx")])
+    else:
+        lat = smd.build_lattice(s.geom, s.L)
     return lat, ctx.lattice(s, lat)
+
+
+def _golden_qset(ctx, s, lat, lid):
+    """The fixture's q set: the DFT grid of a crystal; for a quasi-crystal
+    the direct-sum Lsz x Lsz set of get_qct_SqData."""
+    if s.qcrystal:
+        q, sc = smd.qcrystal_qpoints(lat)
+        return ctx.qset(lid, use_grid=False, qlist=q, list_scale=sc)
+    return ctx.qset(lid, use_grid=True)
 
 
 @pytest.mark.parametrize("name", golden_names("traj_"))
 def test_fp64_200_steps_per_spin(ctx, name):
     s, d = load_golden(name)
-    lat, lid = _upload(ctx, s)
+    lat, lid = _upload(ctx, s, d)
     n = int(d["n"])
     imp = None if "imp" not in d else np.tile(d["imp"], (n, 1))
     fin = ctx.evolve(lid, d["spins0"][:n], s.dtm, s.ntm - 1, imp=imp)
@@ -40,8 +55,8 @@ def test_fp64_200_steps_per_spin(ctx, name):
 @pytest.mark.parametrize("name", golden_names("spec_"))
 def test_fp64_spectrum_equals_reference(ctx, name):
     s, d = load_golden(name)
-    lat, lid = _upload(ctx, s)
-    qid = ctx.qset(lid, use_grid=True)
+    lat, lid = _upload(ctx, s, d)
+    qid = _golden_qset(ctx, s, lat, lid)
     n = int(d["n"])
     imp = None if "imp" not in d else np.tile(d["imp"], (n, 1))
     r = ctx.run(lid, qid, d["spins0"][:n], s.dtm, s.ntm, win=d["window"], imp=imp)

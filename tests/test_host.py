@@ -37,11 +37,23 @@ def test_version_string():
 
 
 @pytest.mark.parametrize("name", golden_names())
-def test_product_lattice_equals_reference_tables(name):
+def test_product_lattice_equals_reference_tables(name, tmp_path):
+    """Crystals: the product's lattice builder against the reference's
+    make_rvecList / make_nborsTable / make_bondList.  Quasi-crystals: the
+    product's table loader on the approximant's files (written back in the
+    reference's binary layouts) and its bond list with ghost neighbours."""
     s, d = load_golden(name)
-    lat = smd.build_lattice(s.geom, s.L)
+    if s.qcrystal:
+        tag = s.size_tag
+        np.asarray(d["rvec"], np.float64).tofile(str(tmp_path / f"sitesList{tag}.bin"))
+        np.concatenate([d["nb1"], d["nb2"], d["nbx"]], axis=1).astype(np.int32).tofile(
+            str(tmp_path / f"nborsList{tag}.bin"))
+        lat = smd.load_qcrystal(str(tmp_path), s.N, s.geom)
+        assert lat.G == s.G and lat.grid_map is None
+    else:
+        lat = smd.build_lattice(s.geom, s.L)
+        assert np.array_equal(lat.grid_map, d["grid_map"])
     assert np.array_equal(lat.rvec, d["rvec"])
-    assert np.array_equal(lat.grid_map, d["grid_map"])
     for a, b in zip(lat.nbrs, (d["nb1"], d["nb2"], d["nbx"])):
         assert np.array_equal(a, b)
     bonds, nb = smd.build_bonds(lat, s.j2_on, s.jx_on)
@@ -136,3 +148,36 @@ def test_sample_file_roundtrip(tmp_path, disorder):
         assert int(imp[0].sum()) == smp.impurity_count(s.N, 0.05)
     else:
         assert imp2 is None
+
+
+def test_qcrystal_qpoints_follow_the_direct_sum_order(oracle_mod):
+    """The direct-sum q set of get_qct_SqData: index j Lsz + i, FFT order
+    along both axes, dq = 8 pi / Lsz, scale 1 / sqrt(N)."""
+    lat = smd.Lattice("Aamman", 14, 239, 14, 1, [8, 3, 8], np.zeros((239, 2)), None,
+                      [np.zeros((239, z), np.int32) for z in (8, 3, 8)])
+    q, sc = smd.qcrystal_qpoints(lat)
+    qo, sco = oracle_mod.qct_qpoints(14, 239)
+    assert np.array_equal(q, qo) and sc == sco
+    dq = 8.0 * np.pi / 14
+    assert np.allclose(q[1], (dq, 0.0)) and np.allclose(q[14], (0.0, dq))
+    assert np.allclose(q[13], (-dq, 0.0)) and np.allclose(q[7], (-7 * dq, 0.0))
+
+
+def test_qcrystal_settings_follow_the_reference_checks():
+    """latSize is the site count, Lsz the even integer below its square root,
+    and a quasi-crystal run needs PBC_OFF = 1 and qct_RemovePBC = 0
+    (Codes_Folder/subrouts.cpp:1105-1114, smd_code.cpp:365-372)."""
+    from classical_mc_and_smd_for_2d_heisenberg_models_b200.settings import SettingsError
+    s = SMDSettings(geom="Aamman", L=1393, NMeas=2000)
+    s.flags["qcrystal"] = 1
+    s.flags["PBC_OFF"] = 1
+    s.validate(check_dwf=False)
+    assert (s.N, s.Lsz, s.G, s.zn) == (1393, 36, 36, (8, 3, 8))
+    assert s.size_tag == "_AppxtSz(1393)"
+    s.flags["qct_RemovePBC"] = 1
+    with pytest.raises(SettingsError):
+        s.validate(check_dwf=False)
+    s.flags["qct_RemovePBC"] = 0
+    s.flags["PBC_OFF"] = 0
+    with pytest.raises(SettingsError):
+        s.validate(check_dwf=False)

@@ -2,13 +2,13 @@
 import numpy as np
 import pytest
 
-from conftest import golden_names, load_golden
+from conftest import golden_lattice, golden_names, load_golden
 
 
 @pytest.mark.parametrize("name", golden_names())
 def test_lattice_tables_match_reference(oracle_mod, name):
     s, d = load_golden(name)
-    lat = oracle_mod.make_lattice(s.geom, s.L)
+    lat = golden_lattice(oracle_mod, s, d)
     assert np.array_equal(lat["rvec"], d["rvec"])
     assert np.array_equal(lat["grid_map"], d["grid_map"])
     for a, b in zip(lat["nbrs"], (d["nb1"], d["nb2"], d["nbx"])):
@@ -21,7 +21,7 @@ def test_lattice_tables_match_reference(oracle_mod, name):
 @pytest.mark.parametrize("name", golden_names("traj_"))
 def test_trajectory_matches_reference(oracle_mod, name):
     s, d = load_golden(name)
-    lat = oracle_mod.make_lattice(s.geom, s.L)
+    lat = golden_lattice(oracle_mod, s, d)
     for k in range(int(d["n"])):
         m = oracle_mod.Model(s, lat, d.get("imp"))
         fin, _ = oracle_mod.evolve(m, d["spins0"][k], s.dtm, s.ntm - 1)
@@ -32,12 +32,17 @@ def test_trajectory_matches_reference(oracle_mod, name):
 @pytest.mark.parametrize("name", golden_names("spec_"))
 def test_spectrum_matches_reference(oracle_mod, name):
     s, d = load_golden(name)
-    lat = oracle_mod.make_lattice(s.geom, s.L)
+    lat = golden_lattice(oracle_mod, s, d)
+    kw = {}
+    if s.qcrystal:
+        # the direct-sum transform of get_qct_SqData over the Lsz x Lsz q set
+        q, sc = oracle_mod.qct_qpoints(s.G, s.N)
+        kw = dict(grid=False, qlist=q, pos=d["rvec"], list_scale=sc)
     acc = 0.0
     accq = 0.0
     for k in range(int(d["n"])):
         m = oracle_mod.Model(s, lat, d.get("imp"))
-        out = oracle_mod.dyn_spectrum(m, d["spins0"][k], s.dtm, s.ntm, win=d["window"])
+        out = oracle_mod.dyn_spectrum(m, d["spins0"][k], s.dtm, s.ntm, win=d["window"], **kw)
         acc = acc + out["spec"]
         accq = accq + out["qss"]
         assert np.max(np.abs(out["final"] - d["final"][k])) <= 1e-15

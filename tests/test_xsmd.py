@@ -32,7 +32,8 @@ def test_spec_binary_layout_round_trip(tmp_path):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["spec_square", "spec_triang", "spec_lieb_disorder"])
+@pytest.mark.parametrize("name", ["spec_square", "spec_triang", "spec_lieb_disorder",
+                                  "spec_qct239_open"])
 def test_driver_reproduces_reference_outputs(tmp_path, name):
     """Settings and sample files written in the reference's formats, the
     window as outBin/winvec.bin: the driver's MC_Bin_SpecData equals the
@@ -52,6 +53,12 @@ def test_driver_reproduces_reference_outputs(tmp_path, name):
     smp.write_sample_file(os.path.join(wd, "outBin", smp.sample_file_name(s)), s,
                           np.asarray(d["spins0"][:n]), imp)
     np.asarray(d["window"], np.float64).tofile(os.path.join(wd, "outBin", "winvec.bin"))
+    if s.qcrystal:
+        # the approximant's tables in the reference's binary layouts
+        tag = s.size_tag
+        np.asarray(d["rvec"], np.float64).tofile(os.path.join(wd, "outBin", f"sitesList{tag}.bin"))
+        tab = np.concatenate([d["nb1"], d["nb2"], d["nbx"]], axis=1).astype(np.int32)
+        tab.tofile(os.path.join(wd, "outBin", f"nborsList{tag}.bin"))
     rep = xsmd.run(wd, dwf_guard=False)
     Q = rep["Q"]
     spec, qss = xsmd.read_spec_bin(rep["spec_file"], Q, s.ntm)
