@@ -29,7 +29,8 @@ EXPORTS = [
     "smd_static_prepass", "smd_evolve", "smd_batch_create", "smd_batch_info", "smd_batch_run",
     "smd_batch_run_device", "smd_batch_free", "smd_submit", "smd_poll", "smd_wait", "smd_cancel",
     "smd_job_info",
-    "smd_serve_shutdown", "smd_evolve_fp64_noalloc", "smd_measure_fma_peak",
+    "smd_serve_shutdown", "smd_mc_run", "smd_mc_colouring", "smd_evolve_fp64_noalloc",
+    "smd_measure_fma_peak",
 ]
 
 
@@ -82,6 +83,14 @@ class NoAllocModel(C.Structure):
 
 
 NOALLOC_SCRATCH_BYTES = 16 << 20
+
+
+class MCDesc(C.Structure):
+    _fields_ = [("lattice", C.c_int), ("n_temps", C.c_int), ("temps", C.POINTER(C.c_double)),
+                ("chains", C.c_int), ("n_therm", C.c_int), ("n_meas", C.c_int),
+                ("cr_skip", C.c_int), ("pt", C.c_int), ("n_micro", C.c_int),
+                ("n_canon", C.c_int), ("n_micro2", C.c_int), ("n_canon2", C.c_int),
+                ("seed", C.c_ulonglong), ("imp", C.POINTER(C.c_int))]
 
 
 class Report(C.Structure):
@@ -146,5 +155,7 @@ def load():
     L.smd_evolve_fp64_noalloc.argtypes = [C.POINTER(NoAllocModel), C.c_int, C.c_double, C.c_int,
                                           vp, vp, vp, vp]
     L.smd_measure_fma_peak.argtypes = [C.c_int, C.c_int, dp]
+    L.smd_mc_run.argtypes = [vp, C.POINTER(MCDesc), dp, dp, dp, ip, C.POINTER(Report)]
+    L.smd_mc_colouring.argtypes = [vp, C.c_int, ip, ip, ip]
     _lib = L
     return L

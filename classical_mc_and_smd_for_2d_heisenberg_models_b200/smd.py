@@ -360,6 +360,50 @@ class Context:
         return Batch(self, members, dt, n_rec, stride, precision, fix_every)
 
     # -- serving
+    def mc_run(self, lattice_id: int, temps, n_therm: int, n_meas: int, cr_skip: int = 1000,
+               chains: int = 1, pt: bool = False, seed: int = 1, spins0=None, imp=None,
+               sweeps=(5, 5, 2, 8), want_samples: bool = True) -> dict:
+        """The MC stage that writes the SMD sample file (smd_mc_run; the
+        reference's Codes_Folder/mc_hm_code.cpp).  temps: the temperature
+        ladder; chains: independent replicas per temperature; sweeps:
+        (nmicro, ncanon, nmicro2, ncanon2).  Returns samples
+        [chains][T][n_rec][N][3], energy [chains][T][n_therm + n_meas] and
+        pt_counts [chains][T][2] (attempts, acceptances)."""
+        lat, _ = self._keep[("lat", lattice_id)]
+        N = lat.N
+        temps = np.ascontiguousarray(temps, np.float64)
+        T = len(temps)
+        d = _lib.MCDesc()
+        d.lattice, d.n_temps = lattice_id, T
+        d.temps = temps.ctypes.data_as(C.POINTER(C.c_double))
+        d.chains, d.n_therm, d.n_meas, d.cr_skip, d.pt = chains, n_therm, n_meas, cr_skip, int(pt)
+        d.n_micro, d.n_canon, d.n_micro2, d.n_canon2 = sweeps
+        d.seed = seed
+        imp_a = None
+        if imp is not None:
+            imp_a = np.ascontiguousarray(np.broadcast_to(imp, (chains, T, N)), np.int32)
+            d.imp = imp_a.ctypes.data_as(C.POINTER(C.c_int))
+        sp = None if spins0 is None else np.ascontiguousarray(spins0, np.float64).reshape(chains, T, N, 3)
+        n_rec = -(-n_meas // cr_skip)
+        samples = np.zeros((chains, T, n_rec, N, 3)) if want_samples and n_rec else None
+        energy = np.zeros((chains, T, n_therm + n_meas))
+        counts = np.zeros((chains, T, 2), np.int32)
+        rep = _lib.Report()
+        self._check(self.lib.smd_mc_run(self.h, C.byref(d), _dp(sp), _dp(samples), _dp(energy),
+                                        _ip(counts), C.byref(rep)), "smd_mc_run")
+        return dict(samples=samples, energy=energy, pt_counts=counts,
+                    report={k: getattr(rep, k) for k, _ in _lib.Report._fields_})
+
+    def mc_colouring(self, lattice_id: int):
+        """The MC sweeps' colour classes: (order [N], class offsets)."""
+        lat, _ = self._keep[("lat", lattice_id)]
+        order = np.zeros(lat.N, np.int32)
+        cst = np.zeros(65, np.int32)
+        n = C.c_int(64)
+        self._check(self.lib.smd_mc_colouring(self.h, lattice_id, _ip(order), _ip(cst), C.byref(n)),
+                    "smd_mc_colouring")
+        return order, cst[: n.value + 1].copy()
+
     def submit(self, lattice_id, qset_id, spins, dt, n_rec, stride=1, precision=SMD_FP64,
                fix_every=1, win=None, imp=None):
         spins = np.ascontiguousarray(spins, np.float64)

@@ -312,6 +312,56 @@ SMD_API int smd_job_info(smd_ctx *ctx, long long job_id, smd_report *rep);
  * smd_ctx_destroy when smd_submit was used). */
 SMD_API void smd_serve_shutdown(smd_ctx *ctx);
 
+/* ---------------------------------------------------------- Monte Carlo */
+
+/* The MC stage that produces the SMD sample file (the reference's xMC_run,
+ * Codes_Folder/mc_hm_code.cpp; one MPI rank per temperature there).  Per MC
+ * step: n_micro overrelaxation sweeps (reflect_aboutVec, subrouts.cpp:
+ * 4956-5004), n_canon heat-bath sweeps (get_hBathSample + get_rotZ2VMat,
+ * subrouts.cpp:5095-5178), the total energy (get_energyValue), then with
+ * pt set a parallel-tempering exchange between neighbouring temperatures
+ * (mc_hm_code.cpp:3010-3125: even pairs on even steps, odd on odd, from step
+ * 101 of the thermalization stage and at every measurement step, a step
+ * after an accepted exchange running n_micro2 / n_canon2 sweeps).  The
+ * measurement stage keeps the configuration of every cr_skip-th step, the
+ * records MC_Bin_SpinField holds (mc_hm_code.cpp:5167-5176).  Sweeps visit
+ * the sites colour class by colour class (a proper colouring of the active
+ * shells' bonds), not in the reference's shuffled order, with a counter-
+ * based generator: the sampled distribution is the same, the draws are
+ * not. */
+typedef struct {
+    int lattice;            /* lattice id */
+    int n_temps;            /* temperatures */
+    const double *temps;    /* [n_temps] */
+    int chains;             /* independent replicas per temperature */
+    int n_therm;            /* NTerm: thermalization steps */
+    int n_meas;             /* NMeas: measurement steps */
+    int cr_skip;            /* crSkip: a record every cr_skip measurement steps */
+    int pt;                 /* ptON */
+    int n_micro, n_canon;   /* 5, 5 in the reference (subrouts.cpp:305-307) */
+    int n_micro2, n_canon2; /* 2, 8: after an accepted exchange (subrouts.cpp:321-322) */
+    unsigned long long seed;
+    const int *imp;         /* [chains][n_temps][N] impurity flags, or NULL */
+} smd_mc_desc;
+
+/* Run the sampler.  spins0 [chains][n_temps][N][3] (host) start states, or
+ * NULL for seeded random unit vectors (IState high_T).  Outputs (host, each
+ * may be NULL):
+ *   samples    [chains][n_temps][ceil(n_meas / cr_skip)][N][3] records, by
+ *              temperature (the replica holding it at that step)
+ *   energy     [chains][n_temps][n_therm + n_meas] total energy after every
+ *              step, by temperature
+ *   pt_counts  [chains][n_temps][2] exchange attempts and acceptances
+ * rep->site_steps counts site updates (replicas x N x steps x sweeps). */
+SMD_API int smd_mc_run(smd_ctx *ctx, const smd_mc_desc *desc, const double *spins0,
+                       double *samples, double *energy, int *pt_counts, smd_report *rep);
+
+/* The sampler's colour classes of a lattice (active shells as uploaded):
+ * order [N] sites grouped by class, cstart [*ncol + 1] class offsets; *ncol
+ * holds the capacity of cstart - 1 on entry and the class count on return.
+ * No counterpart in the reference (its sweeps are sequential). */
+SMD_API int smd_mc_colouring(smd_ctx *ctx, int lattice_id, int *order, int *cstart, int *ncol);
+
 /* ------------------------------------------------- allocation-free entry */
 
 /* Bytes of the static device array behind smd_evolve_fp64_noalloc. */

@@ -96,13 +96,20 @@ int main(int argc, char **argv)
     const string samples = argv[2];
     const long first = atol(argv[3]);
     const long count = atol(argv[4]);
-    bool dump_final = false, dwf_guard = true, outputs = false, prepass = false;
+    bool dump_final = false, dwf_guard = true, outputs = false, prepass = false, mc = false;
+    long mc_therm = 0, mc_meas = 0;
     for (int a = 5; a < argc; a++) {
         string s = argv[a];
         if (s == "--dump-final") dump_final = true;
         if (s == "--no-dwf-guard") dwf_guard = false;
         if (s == "--outputs") outputs = true;
         if (s == "--prepass") prepass = true;
+        if (s == "--mc" && a + 2 < argc) {
+            mc = true;
+            mc_therm = atol(argv[a + 1]);
+            mc_meas = atol(argv[a + 2]);
+            a += 2;
+        }
     }
     if (chdir(workdir.c_str()) != 0) {
         cerr << "cannot enter " << workdir << "\n";
@@ -280,6 +287,77 @@ int main(int argc, char **argv)
         if (tWForm == "hann2") pw = 2;
         if (tWForm == "hann3") pw = 3;
         hannWindow(ntm, pw, tmWinVec);
+    }
+
+    if (mc) {
+        /* The Monte Carlo stage of one rank (no tempering), as
+           mc_hm_code.cpp:2797-2965 runs it: per MC step nmicro
+           overrelaxation sweeps and ncanon heat-bath sweeps over shuffled
+           site lists, then the total energy; from a disordered start
+           (set_initialSpinField, IState high_T) with the reference's own
+           generators (dSFMT seeded with 20240601 + FIRST, rand() seeded with
+           FIRST for the shuffles).  Writes every step's total energy to
+           ref_mc.bin (and a disordered lattice's impurity map to
+           ref_imp.bin) and prints the mean energy per site of the last
+           mc_meas steps. */
+        dSFMT_init(20240601 + (int)first);   /* one stream per run */
+        srand((unsigned)first);
+        if (disOrder) {
+            impField = new int[Ns];
+            make_impurityField(impRatio, flag);
+            ofstream fi("ref_imp.bin", ios::binary);
+            put(fi, impField, (size_t)Ns);
+        }
+        double **spinField = Alloc_dble_array(Ns, 3);
+        string info;
+        set_initialSpinField(0, info, spinField);
+        const double Beta = 1.0 / Temp;
+        int *siteList = new int[Ns];
+        Vec3d spinVec, spinVecNew, locField, unitVec;
+        double RMat[9], EnrgTotal = 0.0, sum = 0.0;
+        vector<double> trace;
+        auto t1 = high_resolution_clock::now();
+        for (long nmc = 0; nmc < mc_therm + mc_meas; nmc++) {
+            for (int k = 0; k < nmicro; k++) {
+                get_shuffledList(Ns, siteList);
+                for (int n = 0; n < Ns; n++) {
+                    const int i = siteList[n];
+                    get_localSpin(i, spinField, spinVec);
+                    get_localField(i, spinField, locField);
+                    reflect_aboutVec(spinVec, locField, spinVecNew);
+                    set_localSpin(i, spinVecNew, spinField);
+                }
+            }
+            for (int k = 0; k < ncanon; k++) {
+                get_shuffledList(Ns, siteList);
+                for (int n = 0; n < Ns; n++) {
+                    const int i = siteList[n];
+                    get_localField(i, spinField, locField);
+                    unitVec = normVec3d(locField);
+                    get_rotZ2VMat(unitVec, RMat);
+                    const double drand1 = dSFMT_getrnum();
+                    const double drand2 = dSFMT_getrnum();
+                    const double tht = 2.0 * pi * drand1;
+                    double z = 0.0;
+                    get_hBathSample(drand2, Beta, locField, z);
+                    const double w = sqrt(1.0 - z * z);
+                    spinVec[0] = w * cos(tht);
+                    spinVec[1] = w * sin(tht);
+                    spinVec[2] = z;
+                    spinVecNew = MxVecProduct(RMat, spinVec);
+                    set_localSpin(i, spinVecNew, spinField);
+                }
+            }
+            get_energyValue(spinField, EnrgTotal);
+            trace.push_back(EnrgTotal);
+            if (nmc >= mc_therm) sum += EnrgTotal;
+        }
+        double ms = duration<double, milli>(high_resolution_clock::now() - t1).count();
+        ofstream f("ref_mc.bin", ios::binary);
+        put(f, trace.data(), trace.size());
+        printf("{\"Ns\": %d, \"T\": %.10g, \"steps\": %ld, \"e_site\": %.17g, \"mc_ms\": %.3f}\n", Ns, Temp,
+               mc_therm + mc_meas, mc_meas > 0 ? sum / mc_meas / Ns : 0.0, ms);
+        return 0;
     }
 
     /* ---- sample file geometry (smd_code.cpp:976-1066) */

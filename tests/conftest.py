@@ -34,9 +34,10 @@ def golden_lattice(oracle_mod, s, d):
 
 def golden_names(prefix=""):
     """Fixture names with the prefix; without one, the trajectory and
-    spectrum cases (the text_ output-stage fixtures have another layout)."""
+    spectrum cases (the text_ output-stage and mc_ Monte Carlo fixtures have
+    other layouts)."""
     names = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, prefix + "*.npz")))
-    return names if prefix else [n for n in names if not n.startswith("text_")]
+    return names if prefix else [n for n in names if not n.startswith(("text_", "mc_"))]
 
 
 @pytest.fixture(scope="session")

@@ -16,7 +16,7 @@ Spectrum cases also get text_<name>.npz: the reference's output stage
 files, autocorrelation) through smd_ref_run --outputs.
 
 Run from the repository root (needs the reference sources at build time):
-    make -C oracle ref && python tests/golden/make_golden.py [--text | --qct]
+    make -C oracle ref && python tests/golden/make_golden.py [--text | --qct | --mc]
 """
 from __future__ import annotations
 
@@ -117,6 +117,66 @@ def run_qct_case(name, folder, N, over, ntm, n, state, sigma, seed, workroot):
     return info
 
 
+# Monte Carlo cases: the reference's MC stage (overrelaxation + heat-bath
+# sweeps, one rank, no tempering) through smd_ref_run --mc, RUNS independent
+# runs per temperature (dSFMT and rand() seeded per run) of THERM + MEAS MC
+# steps; a fixture keeps every run's mean energy per site and, on disordered
+# lattices, every run's impurity map.
+# (name, settings overrides, temperatures, runs, therm, meas, qct table)
+MC_CASES = [
+    ("mc_square_j1j2", dict(geom="square", L=8, J2=0.3), (0.3, 0.8), 8, 1000, 8000, None),
+    ("mc_triang_h_vac", dict(geom="triang", L=6, J2=0.1, h=0.3, imp_ratio=0.1, J1ic=0.5, J2ic=0.2),
+     (0.4,), 8, 1000, 8000, None),
+    ("mc_kagome_xxz", dict(geom="kagome", L=6, J2=0.2, zlamb1=0.8, zlamb2=0.8), (0.25,), 8, 1000, 8000,
+     None),
+    ("mc_qct239", dict(geom="Aamman", L=239, J2=0.3), (0.5,), 8, 1000, 8000, "with_PBC/239"),
+]
+
+
+def run_mc_case(name, over, temps, runs, therm, meas, table, workroot):
+    import shutil
+    import subprocess
+    out = dict(temps=np.array(temps), runs=np.int32(runs), therm=np.int32(therm),
+               meas=np.int32(meas))
+    e_site, imps = [], []
+    for ti, T in enumerate(temps):
+        s = SMDSettings(ntm=16, NMeas=2000, crSkip=1000, T1=T, T2=T, **over)
+        if table:
+            s.flags["qcrystal"] = 1
+            s.flags["PBC_OFF"] = 1
+        wd = os.path.join(workroot, f"{name}_{ti}")
+        s.write(wd)
+        if table:
+            os.makedirs(os.path.join(wd, "outBin"), exist_ok=True)
+            for f in (f"sitesList{s.size_tag}.bin", f"nborsList{s.size_tag}.bin"):
+                shutil.copy(os.path.join(QCT_DIR, table, f), os.path.join(wd, "outBin", f))
+        row, irow = [], []
+        for run in range(runs):
+            r = subprocess.run([os.path.join(ROOT, "oracle", "_ref", "smd_ref_run"), wd, "none",
+                                str(1000 * ti + run + 1), "0", "--no-dwf-guard", "--mc", str(therm),
+                                str(meas)], capture_output=True, text=True)
+            if r.returncode:
+                raise RuntimeError(r.stderr)
+            row.append(json.loads(r.stdout.strip().splitlines()[-1])["e_site"])
+            if s.disorder:
+                irow.append(np.fromfile(os.path.join(wd, "ref_imp.bin"), dtype=np.int32))
+        e_site.append(row)
+        if irow:
+            imps.append(np.stack(irow))
+        if ti == 0:
+            out["settings"] = json.dumps(dataclasses.asdict(s))
+            if table:
+                lat = O.read_ref_lattice(wd)
+                out.update(rvec=lat["rvec"], nb1=lat["nbrs"][0], nb2=lat["nbrs"][1],
+                           nbx=lat["nbrs"][2])
+    out["e_site"] = np.array(e_site)
+    if imps:
+        out["imp"] = np.stack(imps).astype(np.int8)
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+    e = out["e_site"]
+    return [(float(m), float(sd)) for m, sd in zip(e.mean(1), e.std(1, ddof=1) / np.sqrt(runs))]
+
+
 def run_case(name, over, ntm, n, kind, sigma, seed, workroot):
     s = SMDSettings(ntm=ntm, NMeas=1000 * max(n, 2), crSkip=1000, **over)
     s.validate(check_dwf=False)
@@ -191,6 +251,11 @@ def main():
         raise SystemExit("oracle/_ref/smd_ref_run is missing: run `make -C oracle ref` first")
     text_only = "--text" in sys.argv
     qct_only = "--qct" in sys.argv
+    if "--mc" in sys.argv:
+        with tempfile.TemporaryDirectory() as tmp:
+            for c in MC_CASES:
+                print(c[0], run_mc_case(*c, tmp))
+        return
     with tempfile.TemporaryDirectory() as tmp:
         if not text_only:
             for c in QCT_CASES:
