@@ -7,7 +7,7 @@ sample, the per-record projection onto all q, the windowed time transform
 and the sample accumulation of |S(q,w)|^2.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c1|c2|c3|c4] [--no-cpu-baseline]
+                    [--workload c1|c2|c3|c4|mc] [--no-cpu-baseline]
 
 Under torchrun every rank integrates its own 64 samples (weak scaling); the
 sample sums are added across ranks with one NCCL all-reduce per step, the
@@ -686,6 +686,114 @@ def run_batch(args, bw, rank, world):
     }
 
 
+def run_mc(args, rank, world):
+    """The Monte Carlo stage that produces the sample file (smd_mc_run):
+    square L = 64 (N = 4096), J1 = 1, J2 = 0.3, 32 temperatures in
+    [0.2, 1.0] x 4 chains = 128 replicas with parallel tempering, 200
+    thermalization + 800 measurement MC steps of 5 overrelaxation + 5
+    heat-bath sweeps, a record every 100 steps.  One bench step = one such
+    run; the metric is site updates per second (replicas x N x sweeps x
+    steps).  Replicas are independent across ranks (weak scaling)."""
+    import torch
+    from classical_mc_and_smd_for_2d_heisenberg_models_b200 import _lib, smd
+    from classical_mc_and_smd_for_2d_heisenberg_models_b200.settings import SMDSettings
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    s = SMDSettings(geom="square", L=64, J1=1.0, J2=0.3)
+    temps = np.linspace(0.2, 1.0, 32)
+    chains, therm, meas, skip = 4, 200, 800, 100
+    ctx = smd.Context(local)
+    lat = smd.build_lattice(s.geom, s.L)
+    lid = ctx.lattice(s, lat)
+    run = lambda seed: ctx.mc_run(lid, temps, therm, meas, cr_skip=skip, chains=chains, pt=True,
+                                  seed=seed + 7919 * rank)
+    for k in range(args.warmup):
+        run(k + 1)
+    reps, walls = [], []
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            t0 = time.perf_counter()
+            out = run(100 + k)
+            walls.append(time.perf_counter() - t0)
+            reps.append(out["report"])
+    ms_dev = sum(r["ms_device"] for r in reps)
+    updates = sum(r["site_steps"] for r in reps)
+    t = torch.tensor([ms_dev], dtype=torch.float64, device=f"cuda:{local}")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.destroy_process_group()
+    value = updates * world / (float(t.item()) / 1e3)
+    e_site = out["energy"][:, :, therm:].mean(axis=(0, 2)) / lat.N
+    peak64 = fp64_fma_peak(ctx, local)
+    # one site update: the field (6 z flops) and the move (reflection 16,
+    # heat bath about 60 incl. the rotation), averaged over the 5 + 5 sweeps
+    fpu = 6 * 8 + 38
+    ach = fpu * updates / (ms_dev / 1e3) / 1e12
+    ctx.close()
+    R = len(temps) * chains
+    return {
+        "metric": "MC site-updates/s", "value": value, "unit": "site-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_dev / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "seeded random start (IState high_T)",
+        "config": {"workload": f"mc: square L=64 N=4096, J2=0.3, {len(temps)} temperatures in "
+                               f"[0.2, 1.0] x {chains} chains = {R} replicas, parallel tempering, "
+                               f"{therm} + {meas} MC steps of 5 + 5 sweeps, a record every {skip}",
+                   "l2": "replica spins in shared memory (98 KB each)"},
+        "energy_per_site_by_T": [float(x) for x in e_site],
+        "pt_acceptance": float(out["pt_counts"][:, :, 1].sum() / max(1, out["pt_counts"][:, :, 0].sum())),
+        "e2e": {"value": updates * world / sum(walls), "unit": "site-updates/s",
+                "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": int(out["samples"].nbytes + out["energy"].nbytes)},
+        "roofline": {"kernel": "mc_step_kernel", "bound": "fp64", "achieved": ach, "unit": "TFLOP/s",
+                     "peak": peak64, "frac": ach / peak64 if peak64 else None,
+                     "peak_source": "smd_measure_fma_peak (FP64 FMA chains on every SM)",
+                     "algorithmic_flops_per_site_update": fpu},
+        "gpu_launches": int(sum(r["kernel_launches"] for r in reps)),
+        "clocks": clk.summary(),
+    }
+
+
+def fp64_fma_peak(ctx, device):
+    """Measured FP64 FMA peak of the device (TFLOP/s), or None."""
+    import ctypes as C
+    from classical_mc_and_smd_for_2d_heisenberg_models_b200 import _lib
+    v = C.c_double()
+    return v.value if ctx.lib.smd_measure_fma_peak(device, _lib.SMD_FP64, C.byref(v)) == 0 else None
+
+
+def mc_cpu_baseline(args):
+    """The reference's own MC sweeps (smd_ref_run --mc) on the same lattice
+    at one temperature, one single-rank process per host core, 100 MC steps
+    each."""
+    if not reference_available():
+        return {"value": None, "unavailable": "oracle/_ref/smd_ref_run not built"}
+    from classical_mc_and_smd_for_2d_heisenberg_models_b200.settings import SMDSettings
+    procs = ref_procs()
+    s = SMDSettings(geom="square", L=64, J1=1.0, J2=0.3, T1=0.5, T2=0.5, ntm=16)
+    wd = tempfile.mkdtemp(prefix="smd_mc_ref_")
+    s.write(wd)
+    runner = os.path.join(ROOT, "oracle", "_ref", "smd_ref_run")
+    jobs = [subprocess.Popen([runner, wd, "none", str(p + 1), "0", "--no-dwf-guard", "--mc", "0",
+                              "100"], stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
+            for p in range(procs)]
+    ms = []
+    for j in jobs:
+        out, err = j.communicate()
+        if j.returncode != 0:
+            raise RuntimeError(f"reference MC failed: {err.strip()[-300:]}")
+        ms.append(json.loads(out.strip().splitlines()[-1])["mc_ms"])
+    updates = procs * s.N * 100 * 10
+    return {"value": updates / (max(ms) / 1e3), "unit": "site-updates/s", "cores": procs,
+            "kind": "reference",
+            "sample": f"{procs} processes x 100 MC steps (5 + 5 sweeps) of square L=64 at T=0.5"}
+
+
 def cpu_baseline(w, args):
     """Bounded sample of the reference's own CPU code, all host cores."""
     if not reference_available():
@@ -734,7 +842,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "mc"])
     ap.add_argument("--ref-ntm", type=int, default=1025)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
@@ -749,6 +857,20 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     from classical_mc_and_smd_for_2d_heisenberg_models_b200 import workloads
     import dataclasses
+    if args.workload == "mc":
+        if args.impl == "reference":
+            line = mc_cpu_baseline(args) if rank == 0 else None
+            if line is not None:
+                line = dict(line, impl="reference", metric="MC site-updates/s",
+                            e2e={"value": line["value"], "unit": "site-updates/s",
+                                 "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+        else:
+            line = run_mc(args, rank, world)
+            if rank == 0 and world == 1 and not args.no_cpu_baseline:
+                line["cpu_baseline"] = mc_cpu_baseline(args)
+        if rank == 0 and line is not None:
+            print(json.dumps(line))
+        return
     if args.workload == "c3":
         bw = workloads.c3(args.samples or 256)
         # the reference arm and the CPU baseline run the batch's largest lattice

@@ -449,10 +449,15 @@ extern "C" int smd_mc_run(smd_ctx *ctx, const smd_mc_desc *d, const double *spin
     const size_t spin_smem = (size_t)3 * N * sizeof(double);
     P.smem_spins = base_smem + spin_smem <= 200 * 1024 ? 1 : 0;
     const size_t smem = (base_smem + (P.smem_spins ? spin_smem : 0) + 15) & ~size_t(15);
-    const int threads = std::min(1024, std::max(64, (max_class + 31) / 32 * 32));
     const bool gen = d->imp || L.dev.lieb_delta_on;
     auto kern = gen ? mc_step_kernel<true> : mc_step_kernel<false>;
     CK(allow_dynamic_smem(kern), "smem attribute");
+    // a thread per site of the largest class, within the block size the
+    // kernel's registers allow
+    cudaFuncAttributes fa{};
+    CK(cudaFuncGetAttributes(&fa, kern), "kernel attributes");
+    const int tmax = std::max(32, fa.maxThreadsPerBlock / 32 * 32);
+    const int threads = std::min(tmax, std::max(64, (max_class + 31) / 32 * 32));
 
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0), "event");

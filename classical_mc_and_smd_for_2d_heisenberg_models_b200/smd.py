@@ -359,7 +359,7 @@ class Context:
         qset_id, n_samples, imp or None)]."""
         return Batch(self, members, dt, n_rec, stride, precision, fix_every)
 
-    # -- serving
+    # -- Monte Carlo
     def mc_run(self, lattice_id: int, temps, n_therm: int, n_meas: int, cr_skip: int = 1000,
                chains: int = 1, pt: bool = False, seed: int = 1, spins0=None, imp=None,
                sweeps=(5, 5, 2, 8), want_samples: bool = True) -> dict:
@@ -404,6 +404,7 @@ class Context:
                     "smd_mc_colouring")
         return order, cst[: n.value + 1].copy()
 
+    # -- serving
     def submit(self, lattice_id, qset_id, spins, dt, n_rec, stride=1, precision=SMD_FP64,
                fix_every=1, win=None, imp=None):
         spins = np.ascontiguousarray(spins, np.float64)

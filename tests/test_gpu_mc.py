@@ -123,3 +123,15 @@ def test_records_are_unit_spin_fields_that_feed_the_smd_path(ctx, tmp_path):
     qid = ctx.qset(lid)
     r = ctx.run(lid, qid, spins, s.dtm, s.ntm, want_final=False)
     assert np.all(np.isfinite(r.spec)) and r.qss[0] == 1.0
+
+
+def test_large_lattice_runs_with_the_block_size_its_registers_allow(ctx):
+    """Square L = 64 with J2: 4 colour classes of 1024 sites each, more than
+    the kernel's register budget allows threads for; the sampler strides over
+    the class with the largest block it can launch."""
+    s = SMDSettings(geom="square", L=64, J2=0.3)
+    lat = smd.build_lattice(s.geom, s.L)
+    lid = ctx.lattice(s, lat)
+    out = ctx.mc_run(lid, [0.4, 0.8], 5, 10, cr_skip=5, chains=2, pt=True, seed=9)
+    assert np.all(np.isfinite(out["energy"])) and out["samples"].shape == (2, 2, 2, lat.N, 3)
+    assert np.allclose(np.linalg.norm(out["samples"], axis=-1), 1.0, atol=1e-12)
