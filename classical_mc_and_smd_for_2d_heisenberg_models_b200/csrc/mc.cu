@@ -385,6 +385,50 @@ extern "C" int smd_mc_run(smd_ctx *ctx, const smd_mc_desc *d, const double *spin
             for (int c = 0; c < 3; c++) h_spins[k * 3 + c] = v[c] / n;
         }
     }
+    // Colour-major storage: site order[q] lives at position q, so a class is
+    // a contiguous run of positions and its loads and stores are coalesced.
+    // Not for the Lieb d-wave term, whose sign follows the site index parity.
+    const bool cmaj = !L.dev.lieb_delta_on;
+    LatticeDev Ld = L.dev;
+    DevBuf dnbr, dbonds;
+    if (cmaj) {
+        std::vector<int> inv(N);
+        for (int q = 0; q < N; q++) inv[order[q]] = q;
+        std::vector<int> ell((size_t)std::max(L.ztot, 1) * N, -1);
+        for (int s = 0; s < 3; s++) {
+            const std::vector<int> &tb = L.nbr_h[s];
+            if (tb.empty()) continue;
+            const int z = L.zn[s];
+            for (int q = 0; q < N; q++)
+                for (int k = 0; k < z; k++) {
+                    const int j = tb[(size_t)order[q] * z + k];
+                    ell[(size_t)(L.zoff[s] + k) * N + q] = j >= 0 ? inv[j] : -1;
+                }
+        }
+        CK(dnbr.ensure(ell.size() * 4), "cudaMalloc");
+        CK(cudaMemcpy(dnbr.p, ell.data(), ell.size() * 4, cudaMemcpyHostToDevice), "H2D table");
+        Ld.nbr = dnbr.as<int>();
+        if (!Ld.energy_from_field && Ld.nbonds > 0) {
+            std::vector<int4> b((size_t)Ld.nbonds);
+            CK(cudaMemcpy(b.data(), Ld.bonds, b.size() * sizeof(int4), cudaMemcpyDeviceToHost), "D2H bonds");
+            for (int4 &e : b) {
+                e.x = inv[e.x];
+                e.y = inv[e.y];
+            }
+            CK(dbonds.ensure(b.size() * sizeof(int4)), "cudaMalloc");
+            CK(cudaMemcpy(dbonds.p, b.data(), b.size() * sizeof(int4), cudaMemcpyHostToDevice), "H2D bonds");
+            Ld.bonds = dbonds.as<int4>();
+        }
+        std::vector<double> tmp((size_t)N * 3);
+        for (int r = 0; r < R; r++) {
+            double *row = h_spins.data() + (size_t)r * N * 3;
+            for (int q = 0; q < N; q++)
+                for (int c = 0; c < 3; c++) tmp[(size_t)q * 3 + c] = row[(size_t)order[q] * 3 + c];
+            std::copy(tmp.begin(), tmp.end(), row);
+        }
+    }
+    std::vector<int> pos_order(N);   // the class runs in stored positions
+    for (int q = 0; q < N; q++) pos_order[q] = cmaj ? q : order[q];
     std::vector<double> h_beta(R);
     std::vector<int> h_perm(R);
     for (int c = 0; c < C; c++)
@@ -411,12 +455,14 @@ extern "C" int smd_mc_run(smd_ctx *ctx, const smd_mc_desc *d, const double *spin
     std::vector<uint8_t> h_imp;
     if (d->imp) {
         h_imp.resize((size_t)R * N);
-        for (size_t k = 0; k < h_imp.size(); k++) h_imp[k] = d->imp[k] ? 1 : 0;
+        for (int r = 0; r < R; r++)
+            for (int q = 0; q < N; q++)
+                h_imp[(size_t)r * N + q] = d->imp[(size_t)r * N + (cmaj ? order[q] : q)] ? 1 : 0;
         CK(dimp.ensure(h_imp.size()), "cudaMalloc");
         CK(cudaMemcpyAsync(dimp.p, h_imp.data(), h_imp.size(), cudaMemcpyHostToDevice, st), "H2D imp");
     }
     CK(cudaMemcpyAsync(in.p, h_spins.data(), h_spins.size() * 8, cudaMemcpyHostToDevice, st), "H2D spins");
-    CK(cudaMemcpyAsync(dord.p, order.data(), (size_t)N * 4, cudaMemcpyHostToDevice, st), "H2D order");
+    CK(cudaMemcpyAsync(dord.p, pos_order.data(), (size_t)N * 4, cudaMemcpyHostToDevice, st), "H2D order");
     CK(cudaMemcpyAsync(dcst.p, cstart.data(), cstart.size() * 4, cudaMemcpyHostToDevice, st), "H2D classes");
     CK(cudaMemcpyAsync(dbeta.p, h_beta.data(), (size_t)R * 8, cudaMemcpyHostToDevice, st), "H2D beta");
     CK(cudaMemcpyAsync(dperm.p, h_perm.data(), (size_t)R * 4, cudaMemcpyHostToDevice, st), "H2D perm");
@@ -429,7 +475,7 @@ extern "C" int smd_mc_run(smd_ctx *ctx, const smd_mc_desc *d, const double *spin
     CK(cudaStreamSynchronize(st), "sync");
 
     McParams P{};
-    P.L = L.dev;
+    P.L = Ld;
     P.N = N;
     P.order = dord.as<int>();
     P.cstart = dcst.as<int>();
@@ -511,6 +557,17 @@ extern "C" int smd_mc_run(smd_ctx *ctx, const smd_mc_desc *d, const double *spin
         CK(launch_soa_to_aos(drec.as<double>(), dout.as<double>(), R * n_rec, N, st), "soa_to_aos");
         launches++;
         CK(cudaMemcpyAsync(samples, dout.p, (size_t)R * n_rec * 3 * N * 8, cudaMemcpyDeviceToHost, st), "D2H samples");
+        CK(cudaStreamSynchronize(st), "sync");
+        if (cmaj) {
+            // back to the lattice's site order
+            std::vector<double> tmp((size_t)N * 3);
+            for (size_t w = 0; w < (size_t)R * n_rec; w++) {
+                double *row = samples + w * N * 3;
+                for (int q = 0; q < N; q++)
+                    for (int c = 0; c < 3; c++) tmp[(size_t)order[q] * 3 + c] = row[(size_t)q * 3 + c];
+                std::copy(tmp.begin(), tmp.end(), row);
+            }
+        }
     }
     if (energy_out)
         CK(cudaMemcpyAsync(energy_out, d->pt ? dent.p : den.p, (size_t)R * total * 8, cudaMemcpyDeviceToHost, st),
