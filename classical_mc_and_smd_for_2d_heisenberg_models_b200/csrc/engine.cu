@@ -80,6 +80,13 @@ struct SJob {
     std::shared_ptr<Lattice> L;
     std::shared_ptr<QSet> Qs;
     int next_sample = 0, groups_live = 0, vcs = 1, R = 0;
+    // streams mode: the single-job cluster configuration of the job, and the
+    // event after its last enqueued time transform (groups of one job add
+    // into its accumulator one after the other)
+    ClusterTab *ctab = nullptr;
+    int cspt = 0, cthreads = 0;
+    cudaEvent_t ev_fin = nullptr;
+    bool fin_recorded = false;
     size_t acc_bytes = 0;
     DevBuf acc, accq, win, stat;
     Pinned *stage = nullptr;       // spectra, autocorrelation, status, then [n_samples][4] energy stats
@@ -93,7 +100,17 @@ struct Group {
     int chunk = 0;
     int s_begin = 0;   // first sample of the job in this group
     size_t bytes = 0;
+    int lane = -1;     // streams mode: the stream pair running the group
 };
+
+// streams mode: a stream pair (RK at the highest priority, projections at
+// the lowest) with the events that order its three snapshot buffers
+struct Lane {
+    cudaStream_t rk = nullptr, proj = nullptr;
+    cudaEvent_t ev_rk[kSnapBufs]{}, ev_proj[kSnapBufs]{}, done = nullptr;
+    bool busy = false;
+};
+constexpr int kLanes = 16;
 
 struct Engine {
     smd_ctx *parent = nullptr, *ectx = nullptr;
@@ -116,6 +133,18 @@ struct Engine {
     std::vector<int2> h_items[kSnapBufs][2];
     cudaEvent_t ev_rk[kSnapBufs]{}, ev_proj[kSnapBufs]{};
     std::map<long long, int> max_clusters;   // keyed by (prec, zt, csh, smem KiB)
+    // Scheduling.  Streams mode (default): every admitted group runs the
+    // single-job pipeline -- the cluster RK kernel with its job's own
+    // configuration, its projections and its time transform -- enqueued at
+    // admission on a stream pair of its own, so the groups of all jobs in
+    // flight overlap on the device without a common tick.  Tick mode
+    // (SMD_SERVE_MODE=tick): one persistent batch RK launch per tick
+    // advances every group by one chunk.
+    bool streams = true;
+    std::vector<Lane> lanes;
+    int err_rc = SMD_OK;   // a failed enqueue in admit(): the run loop fails the jobs in flight
+    int enqueue_group(Group &g);
+    int reap_groups();
     // SMD_SERVE_TRACE=1: per-tick host and device times on stderr
     bool trace = false;
     cudaEvent_t tr[kSnapBufs][4]{};
@@ -185,11 +214,22 @@ int Engine::start_job(SJob &j)
     probe.S = 1;
     if (j.desc.precision != SMD_FP32 && j.desc.precision != SMD_FP64) return fail(ctx, SMD_EINVAL, "job: precision");
     // records per chunk: about 512 RK steps per tick for every job, so the
-    // work items of a launch take similar times
-    j.R = std::max(8, std::min(128, 512 / std::max(1, j.desc.stride)));
+    // work items of a launch take similar times (tick mode); 128 records
+    // per RK launch, the single-job path's chunk (streams mode)
+    j.R = streams ? std::min(128, j.desc.n_rec)
+                  : std::max(8, std::min(128, 512 / std::max(1, j.desc.stride)));
     probe.R = j.R;
     j.batched = cluster_ok(*j.L) && member_setup(ctx, probe) == SMD_OK;
-    if (j.batched) {
+    if (j.batched && streams) {
+        // the configuration the single-job path takes for this job (a
+        // function of the lattice, precision and the job's sample count, not
+        // of the group sizes, so the job's arithmetic is the same alone and
+        // in any mix)
+        j.ctab = cluster_choice(*j.L, j.desc.precision, j.desc.n_samples, parent->device, &j.cspt,
+                                &j.cthreads);
+        if (!j.ctab) j.batched = false;
+        else j.vcs = j.ctab->P.CS;
+    } else if (j.batched) {
         j.vcs = member_ctas(probe, spt, 18, nullptr);
         if (!j.vcs) j.batched = false;
     }
@@ -210,6 +250,11 @@ int Engine::start_job(SJob &j)
     j.stage = get_pinned((3 * Q * n + n) * 8 + 64 + (size_t)j.desc.n_samples * 32);
     if (!j.stage) return fail(ctx, SMD_ECUDA, "serving: pinned staging");
     used += j.acc_bytes;
+    if (streams) {
+        CK(cudaEventCreateWithFlags(&j.ev_fin, cudaEventDisableTiming), "event");
+        // the lanes' streams read the accumulators and window set up above
+        CK(cudaStreamSynchronize(st), "sync");
+    }
     return SMD_OK;
 }
 
@@ -291,6 +336,12 @@ int Engine::admit()
             continue;
         }
         if ((int)active.size() >= kMaxActive) return admitted;
+        int lane = -1;
+        if (streams) {
+            for (int k = 0; k < (int)lanes.size() && lane < 0; k++)
+                if (!lanes[k].busy) lane = k;
+            if (lane < 0) return admitted;   // every stream pair is running a group
+        }
         // the largest group of the remaining samples that fits the free budget
         auto make = [&](int S) {
             auto m = std::make_unique<Member>();
@@ -308,7 +359,7 @@ int Engine::admit()
             member_setup(ectx, *m);
             m->vcs = j.vcs;
             const int per = kMaxClusterCTAs / j.vcs;   // samples per item at the widest cluster
-            m->Sp = (S + per - 1) / per * per;
+            m->Sp = streams ? S : (S + per - 1) / per * per;
             return m;
         };
         const int left = j.desc.n_samples - j.next_sample;
@@ -348,7 +399,7 @@ int Engine::admit()
         }
         // buffers and inputs of the group
         smd_ctx *ctx = ectx;
-        cudaStream_t st = ectx->s_rk;
+        cudaStream_t st = streams ? lanes[lane].rk : ectx->s_rk;
         if (!j.imp.empty()) {
             const size_t N = m->N;
             m->imp.resize((size_t)m->Sp * N);
@@ -393,11 +444,20 @@ int Engine::admit()
         g.job = &j;
         g.s_begin = j.next_sample;
         g.bytes = bytes;
+        g.lane = lane;
         used += bytes;
         j.next_sample += S;
         j.groups_live++;
         active.push_back(std::move(g));
         admitted++;
+        if (streams) {
+            lanes[lane].busy = true;
+            const int rc = enqueue_group(active.back());
+            if (rc != SMD_OK) {
+                err_rc = rc;
+                return admitted;
+            }
+        }
         if (j.next_sample >= j.desc.n_samples) {
             std::lock_guard<std::mutex> lk(mu);
             queue.pop_front();
@@ -528,6 +588,96 @@ int Engine::do_tick()
     return SMD_OK;
 }
 
+// Streams mode: the group's whole pipeline, enqueued at admission on its
+// lane as the single-job path runs it -- per chunk of R records the cluster
+// RK kernel on the lane's RK stream, then the chunk's projections on its
+// projection stream (three snapshot buffers between the two); after the
+// last chunk the time transform adds into the job's accumulator behind the
+// job's earlier groups, and the group's energy statistics go to the job's
+// staging.
+int Engine::enqueue_group(Group &g)
+{
+    smd_ctx *ctx = ectx;
+    Lane &ln = lanes[g.lane];
+    Member &m = *g.m;
+    SJob &j = *g.job;
+    int launches = 0;
+    for (int c = 0; c < m.nchunks; c++) {
+        const int b = c % kSnapBufs;
+        if (c >= kSnapBufs) CK(cudaStreamWaitEvent(ln.rk, ln.ev_proj[b], 0), "wait");
+        const int rb = c * m.R, re = std::min(m.n_rec, rb + m.R);
+        const RKJob J = member_job(m, rb, re, b);
+        CK(launch_rk_cluster(j.ctab->P, J, m.prec, j.cspt, j.cthreads, ln.rk), "rk cluster kernel");
+        CK(cudaEventRecord(ln.ev_rk[b], ln.rk), "event");
+        CK(cudaStreamWaitEvent(ln.proj, ln.ev_rk[b], 0), "wait");
+        const int rc = member_project(ctx, m, c, ln.proj, &launches);
+        if (rc) return rc;
+        CK(cudaEventRecord(ln.ev_proj[b], ln.proj), "event");
+    }
+    if (j.fin_recorded) CK(cudaStreamWaitEvent(ln.proj, j.ev_fin, 0), "wait");
+    const int rc = member_finish(ctx, m, j.acc.as<double>(), j.accq.as<double>(), ln.proj, &launches);
+    if (rc) return rc;
+    const size_t Q = j.Qs->Q, n = j.desc.n_rec;
+    char *h = static_cast<char *>(j.stage->p) + (3 * Q * n + n) * 8 + 64 + (size_t)g.s_begin * 32;
+    CK(cudaMemcpyAsync(h, m.stats.p, (size_t)m.S * 32, cudaMemcpyDeviceToHost, ln.proj), "D2H stats");
+    CK(cudaEventRecord(j.ev_fin, ln.proj), "event");
+    j.fin_recorded = true;
+    CK(cudaEventRecord(ln.done, ln.proj), "event");
+    g.chunk = m.nchunks;
+    return SMD_OK;
+}
+
+// Streams mode: groups whose lane has finished leave (their buffers go back
+// to the pool, their lane to the free list); a job whose last group is done
+// gets its averages staged for the caller.  Returns the groups reaped, or
+// a negative status.
+int Engine::reap_groups()
+{
+    smd_ctx *ctx = ectx;
+    int done = 0;
+    for (size_t i = 0; i < active.size();) {
+        Group &g = active[i];
+        Lane &ln = lanes[g.lane];
+        const cudaError_t q = cudaEventQuery(ln.done);
+        if (q == cudaErrorNotReady) {
+            i++;
+            continue;
+        }
+        if (q != cudaSuccess) return -cuda_fail(ctx, q, "serving lane");
+        for (DevBuf *d : {&g.m->state, &g.m->s0, &g.m->impd, &g.m->series, &g.m->qss, &g.m->qpart, &g.m->stats,
+                          &g.m->e0, &g.m->gscratch})
+            d->st = ln.proj;
+        for (int b = 0; b < kSnapBufs; b++) {
+            g.m->snap[b].st = ln.proj;
+            g.m->ahi[b].st = ln.proj;
+            g.m->alo[b].st = ln.proj;
+        }
+        SJob &j = *g.job;
+        used -= g.bytes;
+        j.groups_live--;
+        ln.busy = false;
+        active.erase(active.begin() + i);   // releases the member's buffers
+        done++;
+        if (j.groups_live == 0 && j.next_sample >= j.desc.n_samples) {
+            cudaStream_t spr = ectx->s_proj;
+            const size_t Q = j.Qs->Q, n = j.desc.n_rec, ns = 3 * Q * n;
+            const double fc = 1.0 / (double)j.desc.n_samples;   // smd_code.cpp:3596-3611
+            if (launch_scale(j.acc.as<double>(), ns, fc, spr) != cudaSuccess ||
+                launch_scale(j.accq.as<double>(), n, fc, spr) != cudaSuccess)
+                return -cuda_fail(ctx, cudaGetLastError(), "scale");
+            char *h = static_cast<char *>(j.stage->p);
+            cudaError_t e = cudaMemcpyAsync(h, j.acc.p, ns * 8, cudaMemcpyDeviceToHost, spr);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(h + ns * 8, j.accq.p, n * 8, cudaMemcpyDeviceToHost, spr);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(h + (ns + n) * 8, j.stat.p, sizeof(int), cudaMemcpyDeviceToHost, spr);
+            if (e == cudaSuccess) e = cudaEventRecord(j.ev_out, spr);
+            if (e != cudaSuccess) return -cuda_fail(ctx, e, "D2H outputs");
+            j.finishing = true;
+        }
+    }
+    return done;
+}
+
 // Jobs whose outputs have reached the pinned staging: copy to the caller's
 // buffers and report.
 void Engine::reap()
@@ -565,6 +715,8 @@ void Engine::reap()
         used -= j.acc_bytes;
         cudaEventDestroy(j.ev_out);
         j.ev_out = nullptr;
+        if (j.ev_fin) cudaEventDestroy(j.ev_fin);
+        j.ev_fin = nullptr;
         j.finishing = false;
         auto keep = running[i];
         running.erase(running.begin() + i);
@@ -602,6 +754,40 @@ void Engine::run()
         for (int k = 0; k < 4; k++) cudaEventCreate(&tr[b][k]);
     if (const char *e = std::getenv("SMD_SERVE_SPT")) spt = std::atoi(e) == 2 ? 2 : 4;
     threads = rk_batch_threads(SMD_FP32, spt);
+    if (const char *e = std::getenv("SMD_SERVE_MODE")) streams = std::strcmp(e, "tick") != 0;
+    if (streams && crc == SMD_OK) {
+        int lo = 0, hi = 0;
+        cudaDeviceGetStreamPriorityRange(&lo, &hi);
+        lanes.resize(kLanes);
+        for (Lane &ln : lanes) {
+            bool ok = cudaStreamCreateWithPriority(&ln.rk, cudaStreamNonBlocking, hi) == cudaSuccess &&
+                      cudaStreamCreateWithPriority(&ln.proj, cudaStreamNonBlocking, lo) == cudaSuccess &&
+                      cudaEventCreateWithFlags(&ln.done, cudaEventDisableTiming) == cudaSuccess;
+            for (int b = 0; b < kSnapBufs && ok; b++)
+                ok = cudaEventCreateWithFlags(&ln.ev_rk[b], cudaEventDisableTiming) == cudaSuccess &&
+                     cudaEventCreateWithFlags(&ln.ev_proj[b], cudaEventDisableTiming) == cudaSuccess;
+            if (!ok) crc = SMD_ECUDA;
+        }
+    }
+    // a failed launch or copy: every job in flight fails with rc
+    auto fail_in_flight = [&](int rc) {
+        cudaStreamSynchronize(ectx->s_rk);
+        cudaStreamSynchronize(ectx->s_proj);
+        for (Lane &ln : lanes) {
+            cudaStreamSynchronize(ln.rk);
+            cudaStreamSynchronize(ln.proj);
+            ln.busy = false;
+        }
+        smd_copy_error(parent, ectx, 0);
+        for (auto &g : active) g.job->groups_live = -1;
+        active.clear();
+        for (auto &jp : running) {
+            used -= jp->acc_bytes;
+            finish_job(*jp, rc);
+        }
+        running.clear();
+        used = 0;
+    };
     for (;;) {
         {
             std::unique_lock<std::mutex> lk(mu);
@@ -619,23 +805,26 @@ void Engine::run()
             done_cv.notify_all();
             continue;
         }
-        admit();
+        const int admitted = admit();
+        if (err_rc != SMD_OK) {
+            fail_in_flight(err_rc);
+            err_rc = SMD_OK;
+            continue;
+        }
+        if (streams) {
+            const int n = reap_groups();
+            if (n < 0) {
+                fail_in_flight(-n);
+                continue;
+            }
+            reap();
+            // nothing finished and nothing new: let the lanes run
+            if (n == 0 && admitted == 0) std::this_thread::sleep_for(std::chrono::microseconds(100));
+            continue;
+        }
         if (!active.empty()) {
             int rc = do_tick();
-            if (rc != SMD_OK) {
-                // a launch failed: fail the jobs in flight
-                cudaStreamSynchronize(ectx->s_rk);
-                cudaStreamSynchronize(ectx->s_proj);
-                smd_copy_error(parent, ectx, 0);
-                for (auto &g : active) g.job->groups_live = -1;
-                active.clear();
-                for (auto &jp : running) {
-                    used -= jp->acc_bytes;
-                    finish_job(*jp, rc);
-                }
-                running.clear();
-                used = 0;
-            }
+            if (rc != SMD_OK) fail_in_flight(rc);
         } else if (!running.empty()) {
             // only outputs in flight: wait for the oldest
             for (auto &jp : running)
@@ -647,6 +836,17 @@ void Engine::run()
         reap();
     }
     cudaStreamSynchronize(ectx ? ectx->s_proj : nullptr);
+    for (Lane &ln : lanes) {
+        if (ln.rk) cudaStreamSynchronize(ln.rk);
+        if (ln.proj) cudaStreamSynchronize(ln.proj);
+        for (int b = 0; b < kSnapBufs; b++) {
+            if (ln.ev_rk[b]) cudaEventDestroy(ln.ev_rk[b]);
+            if (ln.ev_proj[b]) cudaEventDestroy(ln.ev_proj[b]);
+        }
+        if (ln.done) cudaEventDestroy(ln.done);
+        if (ln.rk) cudaStreamDestroy(ln.rk);
+        if (ln.proj) cudaStreamDestroy(ln.proj);
+    }
     for (int b = 0; b < kSnapBufs; b++) {
         for (int p = 0; p < 2; p++) d_items[b][p].release();
         d_queue[b].release();

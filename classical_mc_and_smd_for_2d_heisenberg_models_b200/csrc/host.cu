@@ -684,6 +684,45 @@ int project_chunk(smd_ctx *ctx, const ProjArgs &a, cudaStream_t st, int *launche
     return SMD_OK;
 }
 
+// Cluster size and thread shape for a job.  Lattices the cluster kernel does
+// not cover (bond-list energies, the Lieb d-wave term, impurities with
+// non-zero couplings) keep the single-CTA kernel.  Otherwise the smallest
+// cluster that puts at least ~85% of the SMs to work is taken, within the
+// shared-memory and register limits; SMD_CLUSTER_CTAS forces a size.
+ClusterTab *cluster_choice(Lattice &L, int prec, int n_samples, int device, int *spt_out, int *threads_out)
+{
+    if (!cluster_ok(L)) return nullptr;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    int forced = 0;
+    if (const char *e = std::getenv("SMD_CLUSTER_CTAS")) forced = std::atoi(e);
+    ClusterTab *best = nullptr;
+    const int sizes[] = {1, 2, 4, 8, 16};
+    for (int CS : sizes) {
+        if (forced && CS != forced) continue;
+        if (!forced && CS > 1 && L.N / CS < 96) break;
+        ClusterTab *t = cluster_tables(L, CS);
+        if (!t) continue;
+        int spt = 0;
+        // sites per thread: the fewest that fit a block (SMD_RK_SPT forces one)
+        int force_spt = 0;
+        if (const char *e = std::getenv("SMD_RK_SPT")) force_spt = std::atoi(e);
+        for (int s : {1, 2, 4})
+            if ((!force_spt || s == force_spt) && s * rk_cluster_maxt(prec, s) >= t->P.n_own_max) {
+                spt = s;
+                break;
+            }
+        if (!spt) continue;
+        if (rk_cluster_smem(t->P, prec) > 227 * 1024) continue;
+        best = t;
+        *spt_out = spt;
+        *threads_out = std::min(std::max(32, (t->P.n_own_max + spt - 1) / spt + 31) / 32 * 32,
+                                rk_cluster_maxt(prec, spt));
+        if (forced || (long long)n_samples * CS >= (long long)(0.85 * sms)) break;
+    }
+    return best;
+}
+
 }  // namespace smdh
 
 namespace {
@@ -699,43 +738,9 @@ struct JobGeom {
 };
 
 
-// Cluster size and thread shape for a job.  Lattices the cluster kernel does
-// not cover (bond-list energies, the Lieb d-wave term, impurities with
-// non-zero couplings) keep the single-CTA kernel.  Otherwise the smallest
-// cluster that puts at least ~85% of the SMs to work is taken, within the
-// shared-memory and register limits; SMD_CLUSTER_CTAS forces a size.
 void choose_cluster(smd_ctx *ctx, JobGeom &g, int n_samples)
 {
-    Lattice &L = *g.L;
-    g.ctab = nullptr;
-    if (!cluster_ok(L)) return;
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-    int forced = 0;
-    if (const char *e = std::getenv("SMD_CLUSTER_CTAS")) forced = std::atoi(e);
-    const int sizes[] = {1, 2, 4, 8, 16};
-    for (int CS : sizes) {
-        if (forced && CS != forced) continue;
-        if (!forced && CS > 1 && L.N / CS < 96) break;
-        ClusterTab *t = cluster_tables(L, CS);
-        if (!t) continue;
-        int spt = 0;
-        // sites per thread: the fewest that fit a block (SMD_RK_SPT forces one)
-        int force_spt = 0;
-        if (const char *e = std::getenv("SMD_RK_SPT")) force_spt = std::atoi(e);
-        for (int s : {1, 2, 4})
-            if ((!force_spt || s == force_spt) && s * rk_cluster_maxt(g.prec, s) >= t->P.n_own_max) {
-                spt = s;
-                break;
-            }
-        if (!spt) continue;
-        if (rk_cluster_smem(t->P, g.prec) > 227 * 1024) continue;
-        g.ctab = t;
-        g.spt = spt;
-        g.threads = std::max(32, (t->P.n_own_max + spt - 1) / spt + 31) / 32 * 32;
-        g.threads = std::min(g.threads, rk_cluster_maxt(g.prec, spt));
-        if (forced || (long long)n_samples * CS >= (long long)(0.85 * sms)) return;
-    }
+    g.ctab = cluster_choice(*g.L, g.prec, n_samples, ctx->device, &g.spt, &g.threads);
 }
 
 int prepare(smd_ctx *ctx, const smd_job_desc *job, JobGeom &g)

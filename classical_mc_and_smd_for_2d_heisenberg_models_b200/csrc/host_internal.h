@@ -176,6 +176,11 @@ std::shared_ptr<QSet> find_qset(smd_ctx *ctx, int id);
 // Whether the cluster kernel covers the lattice (field-identity energies,
 // no Lieb d-wave term, impurities only as vacancies).
 bool cluster_ok(const Lattice &L);
+// Cluster partition, sites per thread and block size the single-job path
+// takes for a lattice, precision and sample count: the smallest cluster
+// that puts about 85 % of the SMs to work within the shared-memory and
+// register limits.  Null when the lattice needs the single-CTA kernel.
+ClusterTab *cluster_choice(Lattice &L, int prec, int n_samples, int device, int *spt, int *threads);
 
 // Projection of records [rb, re) of W samples from a snapshot buffer
 // ([W][R][3][N] of the precision's type) into the windowed time series;
