@@ -150,7 +150,7 @@ class ClockSampler:
 
 # ------------------------------------------------------------- serving
 
-def serving_leg(ctx, n_jobs: int, seed: int, fp64: bool = True):
+def serving_leg(device: int, n_jobs: int, seed: int, fp64: bool = True):
     """A stream of serving-workload jobs (workloads.c5_stream: five
     geometries, N log-uniform in [256, 16384], 16-256 samples, 2^12-2^15 RK
     steps, 1024 records, FP32 form) through the continuous-batching engine
@@ -161,87 +161,104 @@ def serving_leg(ctx, n_jobs: int, seed: int, fp64: bool = True):
     FP64 spectra each served result's DSSF rel-L2 is taken against and one
     denominator of the 4x target (FP64 device time, no serving overhead); the
     same jobs served as one FP64 burst through the engine give the like-for-
-    like denominator."""
+    like denominator.  Each phase runs in a context of its own, so the
+    buffers one phase grew do not hold device memory the next needs."""
     from classical_mc_and_smd_for_2d_heisenberg_models_b200 import _lib, smd, workloads
     jobs = workloads.c5_stream(n_jobs, seed)
-    prepared = []
-    for w in jobs:
-        s = w.settings
-        lat = smd.build_lattice(s.geom, s.L)
-        lid = ctx.lattice(s, lat)
-        qid = ctx.qset(lid)
-        spins, imp = workloads.make_inputs(w)
-        imp_arr = None if imp is None else np.ascontiguousarray(imp, np.int32)
-        win = smd.window(w.window, w.n_rec)
-        prepared.append((w, lid, qid, spins, imp_arr, win))
-    site_steps = sum(w.settings.N * w.n_samples * w.steps for w, *_ in prepared)
+    site_steps = sum(w.settings.N * w.n_samples * w.steps for w in jobs)
 
-    def submit(p, fp64_plain=False):
-        w, lid, qid, spins, imp_arr, win = p
-        if fp64_plain:
-            return ctx.submit(lid, qid, spins, w.settings.dtm, w.n_rec, stride=w.stride,
-                              precision=_lib.SMD_FP64, fix_every=1, win=win, imp=imp_arr)
-        return ctx.submit(lid, qid, spins, w.settings.dtm, w.n_rec, stride=w.stride,
-                          precision=w.precision, fix_every=w.fix_every, win=win, imp=imp_arr)
+    def prepare(ctx):
+        out = []
+        for w in jobs:
+            s = w.settings
+            lat = smd.build_lattice(s.geom, s.L)
+            lid = ctx.lattice(s, lat)
+            qid = ctx.qset(lid)
+            spins, imp = workloads.make_inputs(w)
+            imp_arr = None if imp is None else np.ascontiguousarray(imp, np.int32)
+            out.append((w, lid, qid, spins, imp_arr, smd.window(w.window, w.n_rec)))
+        return out
 
-    # warm-up burst (untimed): the engine's memory pool, lattice tables,
-    # time plans and pinned staging are set up on first use
-    for j in [submit(p) for p in prepared]:
-        ctx.wait(j)
-    # burst: every job queued at once; the makespan gives the service rate
-    t0 = time.perf_counter()
-    ids = [submit(p) for p in prepared]
-    burst = [ctx.wait(j) for j in ids]
-    makespan = time.perf_counter() - t0
-    infos = [ctx.job_info(j) for j in ids]
-    rate = 0.7 * len(prepared) / makespan
-    rng = np.random.default_rng(seed + 1)
-    gaps = rng.exponential(1.0 / rate, size=len(prepared))
-    t0 = time.perf_counter()
-    ids, t_next = [], 0.0
-    for p, g in zip(prepared, gaps):
-        t_next += g
-        dt = t0 + t_next - time.perf_counter()
-        if dt > 0:
-            time.sleep(dt)
-        ids.append(submit(p))
-    lat = np.array([ctx.wait(j)[2] for j in ids])
-    wall = time.perf_counter() - t0
-    out = {"jobs": len(prepared), "arrivals": "Poisson", "rate_jobs_per_s": rate,
-           "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-           "max_ms": float(lat.max()), "site_steps": float(site_steps),
-           "burst_makespan_s": makespan, "served_site_steps_per_s": site_steps / makespan,
-           "energy_drift_per_site": {"max": max(i["drift_max"] for i in infos),
-                                     "final": max(i["drift_final"] for i in infos)},
-           "sample": f"{len(prepared)} jobs of the serving mix (5 geometries, N log-uniform in "
-                     f"[256, 16384], 16-256 samples, 2^12-2^15 RK steps at the stride giving "
-                     f"1024 records, 0-10 % vacancies, grid q, FP32 form), Poisson at 70 % of "
-                     f"the burst service rate; stream wall time {wall:.1f} s",
-           "job_shapes": [f"{w.settings.geom} N={w.settings.N} S={w.n_samples} "
-                          f"steps={w.steps}" for w, *_ in prepared]}
+    def fp64_solo(ctx, p, spins=None):
+        w, lid, qid, sp, imp_arr, win = p
+        return ctx.run(lid, qid, sp if spins is None else spins, w.settings.dtm, w.n_rec,
+                       stride=w.stride, precision=_lib.SMD_FP64, fix_every=1, win=win, imp=imp_arr,
+                       want_final=False)
+
+    # the FP64 plain form one job at a time through smd_run: device time and spectra
+    ms64, spec64 = 0.0, []
     if fp64:
-        # the FP64 plain form served the same way (one burst through the
-        # engine): the like-for-like denominator of the served form
-        t0 = time.perf_counter()
-        for j in [submit(p, fp64_plain=True) for p in prepared]:
+        with smd.Context(device) as c64:
+            for p in prepare(c64):
+                r = fp64_solo(c64, p)
+                ms64 += r.report["ms_device"]
+                spec64.append(r.spec)
+
+    out = {}
+    with smd.Context(device) as ctx:
+        prepared = prepare(ctx)
+
+        def submit(p, fp64_plain=False):
+            w, lid, qid, spins, imp_arr, win = p
+            prec, fix = (_lib.SMD_FP64, 1) if fp64_plain else (w.precision, w.fix_every)
+            return ctx.submit(lid, qid, spins, w.settings.dtm, w.n_rec, stride=w.stride,
+                              precision=prec, fix_every=fix, win=win, imp=imp_arr)
+
+        # warm-up burst (untimed): the engine's memory pool, lattice tables,
+        # time plans and pinned staging are set up on first use
+        for j in [submit(p) for p in prepared]:
             ctx.wait(j)
-        out["fp64_plain_served_site_steps_per_s"] = site_steps / (time.perf_counter() - t0)
-        out["speedup_vs_fp64_plain_served"] = (out["served_site_steps_per_s"] /
-                                               out["fp64_plain_served_site_steps_per_s"])
-        ms64, rels, floors = 0.0, [], []
-        for (w, lid, qid, spins, imp_arr, win), (spec, _, _) in zip(prepared, burst):
-            kw = dict(stride=w.stride, precision=_lib.SMD_FP64, fix_every=1, win=win,
-                      imp=imp_arr, want_final=False)
-            r = ctx.run(lid, qid, spins, w.settings.dtm, w.n_rec, **kw)
-            ms64 += r.report["ms_device"]
-            rels.append(rel_l2(spec, r.spec))
-            floor = None
-            if rels[-1] > 1e-3:
-                # a chaotic job: the FP64 form's own difference under one FP32
-                # rounding of its inputs
-                pert = workloads.tangent_perturb(spins, workloads.FP32_ROUNDOFF, 11)
-                floor = rel_l2(ctx.run(lid, qid, pert, w.settings.dtm, w.n_rec, **kw).spec, r.spec)
-            floors.append(floor)
+        # burst: every job queued at once; the makespan gives the service rate
+        t0 = time.perf_counter()
+        ids = [submit(p) for p in prepared]
+        burst = [ctx.wait(j) for j in ids]
+        makespan = time.perf_counter() - t0
+        infos = [ctx.job_info(j) for j in ids]
+        rate = 0.7 * len(prepared) / makespan
+        rng = np.random.default_rng(seed + 1)
+        gaps = rng.exponential(1.0 / rate, size=len(prepared))
+        t0 = time.perf_counter()
+        ids, t_next = [], 0.0
+        for p, g in zip(prepared, gaps):
+            t_next += g
+            dt = t0 + t_next - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            ids.append(submit(p))
+        lat = np.array([ctx.wait(j)[2] for j in ids])
+        wall = time.perf_counter() - t0
+        out = {"jobs": len(prepared), "arrivals": "Poisson", "rate_jobs_per_s": rate,
+               "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+               "max_ms": float(lat.max()), "site_steps": float(site_steps),
+               "burst_makespan_s": makespan, "served_site_steps_per_s": site_steps / makespan,
+               "energy_drift_per_site": {"max": max(i["drift_max"] for i in infos),
+                                         "final": max(i["drift_final"] for i in infos)},
+               "sample": f"{len(prepared)} jobs of the serving mix (5 geometries, N log-uniform in "
+                         f"[256, 16384], 16-256 samples, 2^12-2^15 RK steps at the stride giving "
+                         f"1024 records, 0-10 % vacancies, grid q, FP32 form), Poisson at 70 % of "
+                         f"the burst service rate; stream wall time {wall:.1f} s",
+               "job_shapes": [f"{w.settings.geom} N={w.settings.N} S={w.n_samples} "
+                              f"steps={w.steps}" for w, *_ in prepared]}
+        if fp64:
+            # the FP64 plain form served the same way (one burst through the
+            # engine): the like-for-like denominator of the served form
+            t0 = time.perf_counter()
+            for j in [submit(p, fp64_plain=True) for p in prepared]:
+                ctx.wait(j)
+            out["fp64_plain_served_site_steps_per_s"] = site_steps / (time.perf_counter() - t0)
+            out["speedup_vs_fp64_plain_served"] = (out["served_site_steps_per_s"] /
+                                                   out["fp64_plain_served_site_steps_per_s"])
+    if fp64:
+        rels = [rel_l2(spec, s64) for (spec, _, _), s64 in zip(burst, spec64)]
+        floors = [None] * len(rels)
+        if max(rels) > 1e-3:
+            # chaotic jobs: the FP64 form's own difference under one FP32
+            # rounding of its inputs
+            with smd.Context(device) as cf:
+                for k, p in enumerate(prepare(cf)):
+                    if rels[k] > 1e-3:
+                        pert = workloads.tangent_perturb(p[3], workloads.FP32_ROUNDOFF, 11)
+                        floors[k] = rel_l2(fp64_solo(cf, p, pert).spec, spec64[k])
         out["fp64_plain_site_steps_per_s"] = site_steps / (ms64 / 1e3)
         out["speedup_vs_fp64_plain"] = out["served_site_steps_per_s"] / out["fp64_plain_site_steps_per_s"]
         out["dssf_rel_l2_vs_fp64"] = {
@@ -415,9 +432,6 @@ def run_ours(args, w, rank, world):
     spec32 = d_spec.double().cpu().numpy().copy()
 
     # ---- serving: bounded job stream with p50 / p99 latency (rank 0's queue)
-    serving = None
-    if rank == 0 and not args.no_serving:
-        serving = serving_leg(ctx, args.serving_jobs, 0x5eed05)
     h2d = spins.nbytes + win.nbytes
     d2h = 3 * Q * n * 8 + n * 8
 
@@ -494,6 +508,11 @@ def run_ours(args, w, rank, world):
     if dist is not None:
         dist.destroy_process_group()
     ctx.close()
+
+    # ---- serving: the C5-shaped job stream (rank 0), in contexts of its own
+    serving = None
+    if rank == 0 and not args.no_serving:
+        serving = serving_leg(local, args.serving_jobs, 0x5eed05)
 
     line = None
     if rank == 0:

@@ -110,7 +110,7 @@ struct Lane {
     cudaEvent_t ev_rk[kSnapBufs]{}, ev_proj[kSnapBufs]{}, done = nullptr;
     bool busy = false;
 };
-constexpr int kLanes = 16;
+constexpr int kLanes = 16;   // stream pairs (SMD_SERVE_LANES overrides)
 
 struct Engine {
     smd_ctx *parent = nullptr, *ectx = nullptr;
@@ -758,7 +758,9 @@ void Engine::run()
     if (streams && crc == SMD_OK) {
         int lo = 0, hi = 0;
         cudaDeviceGetStreamPriorityRange(&lo, &hi);
-        lanes.resize(kLanes);
+        int nl = kLanes;
+        if (const char *e = std::getenv("SMD_SERVE_LANES")) nl = std::max(1, std::min(kMaxActive, std::atoi(e)));
+        lanes.resize(nl);
         for (Lane &ln : lanes) {
             bool ok = cudaStreamCreateWithPriority(&ln.rk, cudaStreamNonBlocking, hi) == cudaSuccess &&
                       cudaStreamCreateWithPriority(&ln.proj, cudaStreamNonBlocking, lo) == cudaSuccess &&
@@ -893,6 +895,14 @@ int job_state(Engine *e, long long id, double *latency_ms)
 }
 
 }  // namespace
+
+void smdh::engine_trim(smd_ctx *ctx)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_engines.find(ctx);
+    if (it == g_engines.end() || !it->second->pool) return;
+    cudaMemPoolTrimTo(it->second->pool, 0);
+}
 
 extern "C" void smd_serve_shutdown(smd_ctx *ctx)
 {

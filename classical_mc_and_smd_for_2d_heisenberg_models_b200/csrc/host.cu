@@ -795,8 +795,28 @@ int prepare(smd_ctx *ctx, const smd_job_desc *job, JobGeom &g)
                        5 * sizeof(double) + (size_t)g.n_rec * kMaxClusterCTAs * sizeof(double) +
                        (large ? grid_large_scratch(g.Qs->G, g.R, g.prec == SMD_FP64 ? 0 : 1) : 0);
     const size_t fixed = 3 * (size_t)g.Q * g.n_rec * sizeof(double) + (64u << 20);
-    if (ctx->budget <= fixed + per) return fail(ctx, SMD_ENOMEM_ADMIT, "job: one sample exceeds the HBM budget");
-    size_t W = (ctx->budget - fixed) / per;
+    // the budget, and no more than the device can give now: its free memory
+    // plus the job buffers this context holds (they are reallocated), less
+    // a reserve; the serving engine's unused pooled memory is returned first
+    // when that is short
+    size_t budget = ctx->budget;
+    auto avail_now = [&]() -> size_t {
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return ctx->budget;
+        size_t held = ctx->state.bytes + ctx->s0.bytes + ctx->imp.bytes + ctx->series.bytes + ctx->qss.bytes +
+                      ctx->qpart.bytes + ctx->stats.bytes + ctx->e0.bytes + ctx->gscratch.bytes;
+        for (int b = 0; b < kSnapBufs; b++) held += ctx->snap[b].bytes + ctx->ahi[b].bytes + ctx->alo[b].bytes;
+        const size_t reserve = (size_t)1 << 30;
+        return fr + held > reserve ? fr + held - reserve : 0;
+    };
+    size_t avail = avail_now();
+    if (avail < budget) {
+        engine_trim(ctx);
+        avail = avail_now();
+    }
+    budget = std::min(budget, avail);
+    if (budget <= fixed + per) return fail(ctx, SMD_ENOMEM_ADMIT, "job: one sample exceeds the free HBM");
+    size_t W = (budget - fixed) / per;
     W = std::min<size_t>(W, (size_t)job->n_samples);
     W = std::min<size_t>(W, 65535);
     g.W = (int)W;
@@ -812,18 +832,30 @@ int run_device(smd_ctx *ctx, const smd_job_desc *job, const JobGeom &g, const do
     const int N = g.N, Q = g.Q, nqb = g.nqb, n_rec = g.n_rec, R = g.R, W = g.W;
     Lattice &L = *g.L;
     QSet &Qs = *g.Qs;
-    CK(ctx->state.ensure((size_t)W * 3 * N * sizeof(double)), "cudaMalloc state");
-    CK(ctx->s0.ensure((size_t)W * 3 * N * sizeof(double)), "cudaMalloc s0");
-    CK(ctx->imp.ensure((size_t)W * N), "cudaMalloc imp");
-    for (int b = 0; b < kSnapBufs; b++)
-        CK(ctx->snap[b].ensure((size_t)W * R * 3 * N * g.elem), "cudaMalloc snap");
-    CK(ctx->series.ensure((size_t)W * 3 * n_rec * nqb * 16), "cudaMalloc series");
-    CK(ctx->qss.ensure((size_t)W * n_rec * sizeof(double)), "cudaMalloc qss");
-    if (g.ctab)
-        CK(ctx->qpart.ensure((size_t)W * n_rec * g.ctab->P.CS * sizeof(double)), "cudaMalloc qpart");
-    CK(ctx->stats.ensure((size_t)W * 4 * sizeof(double)), "cudaMalloc stats");
-    CK(ctx->e0.ensure((size_t)W * sizeof(double)), "cudaMalloc e0");
-    CK(ctx->status.ensure(sizeof(int)), "cudaMalloc status");
+    // the job's buffers; when the device is short, the serving engine's
+    // pooled memory that no group holds is returned to it and the buffers
+    // are tried once more
+    auto alloc_all = [&]() -> cudaError_t {
+        cudaError_t e = ctx->state.ensure((size_t)W * 3 * N * sizeof(double));
+        if (e == cudaSuccess) e = ctx->s0.ensure((size_t)W * 3 * N * sizeof(double));
+        if (e == cudaSuccess) e = ctx->imp.ensure((size_t)W * N);
+        for (int b = 0; b < kSnapBufs && e == cudaSuccess; b++)
+            e = ctx->snap[b].ensure((size_t)W * R * 3 * N * g.elem);
+        if (e == cudaSuccess) e = ctx->series.ensure((size_t)W * 3 * n_rec * nqb * 16);
+        if (e == cudaSuccess) e = ctx->qss.ensure((size_t)W * n_rec * sizeof(double));
+        if (e == cudaSuccess && g.ctab) e = ctx->qpart.ensure((size_t)W * n_rec * g.ctab->P.CS * sizeof(double));
+        if (e == cudaSuccess) e = ctx->stats.ensure((size_t)W * 4 * sizeof(double));
+        if (e == cudaSuccess) e = ctx->e0.ensure((size_t)W * sizeof(double));
+        if (e == cudaSuccess) e = ctx->status.ensure(sizeof(int));
+        return e;
+    };
+    cudaError_t ae = alloc_all();
+    if (ae == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        engine_trim(ctx);
+        ae = alloc_all();
+    }
+    CK(ae, "cudaMalloc job buffers");
     CK(cudaMemsetAsync(ctx->status.p, 0, sizeof(int), ctx->s_rk), "memset");
     const bool gen = L.lieb_delta || job->imp;
     std::vector<double> stats_h;

@@ -176,6 +176,10 @@ std::shared_ptr<QSet> find_qset(smd_ctx *ctx, int id);
 // Whether the cluster kernel covers the lattice (field-identity energies,
 // no Lieb d-wave term, impurities only as vacancies).
 bool cluster_ok(const Lattice &L);
+// Return the serving engine's pooled device memory that no sample group
+// holds (a no-op without an engine), for a context's own jobs when the
+// device is short.
+void engine_trim(smd_ctx *ctx);
 // Cluster partition, sites per thread and block size the single-job path
 // takes for a lattice, precision and sample count: the smallest cluster
 // that puts about 85 % of the SMs to work within the shared-memory and
