@@ -7,7 +7,7 @@ sample, the per-record projection onto all q, the windowed time transform
 and the sample accumulation of |S(q,w)|^2.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c1|c2|c3|c4|mc] [--no-cpu-baseline]
+                    [--workload c1|c2|c3|c4|c5|mc] [--no-cpu-baseline]
 
 Under torchrun every rank integrates its own 64 samples (weak scaling); the
 sample sums are added across ranks with one NCCL all-reduce per step, the
@@ -874,7 +874,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "mc"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "mc"])
     ap.add_argument("--ref-ntm", type=int, default=1025)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
@@ -889,6 +889,30 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     from classical_mc_and_smd_for_2d_heisenberg_models_b200 import workloads
     import dataclasses
+    if args.workload == "c5":
+        # the served form alone: the C5-shaped job stream through the engine
+        line = None
+        if rank == 0:
+            import torch
+            local = int(os.environ.get("LOCAL_RANK", "0"))
+            torch.cuda.set_device(local)
+            if args.impl == "reference":
+                line = {"impl": "reference", "unavailable": "the serving stream has no counterpart "
+                        "in the reference (one job per process); its CPU code is timed by the "
+                        "c1-c4 workloads"}
+            else:
+                with ClockSampler(local) as clk:
+                    sv = serving_leg(local, args.serving_jobs, 0x5eed05, fp64=not args.no_fp64)
+                line = {"metric": METRIC + " (served)", "value": sv["served_site_steps_per_s"],
+                        "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": 1,
+                        "ms_per_step": sv["burst_makespan_s"] * 1e3, "higher_is_better": True,
+                        "scaling": "weak", "vs_baseline": None,
+                        "dtype": "f32 stages / f64 master+energy", "data": "synthetic (C5 job mix)",
+                        "config": {"workload": "c5: " + sv["sample"]},
+                        "serving": sv, "clocks": clk.summary()}
+        if line is not None:
+            print(json.dumps(line))
+        return
     if args.workload == "mc":
         if args.impl == "reference":
             line = mc_cpu_baseline(args) if rank == 0 else None
