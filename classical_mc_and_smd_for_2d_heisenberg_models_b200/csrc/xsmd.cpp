@@ -111,7 +111,7 @@ struct Settings {
     double dtm = 0.01;
     std::string window;
     double imp_ratio = 0, J1ic = 0, J2ic = 0, JXic = 0, J1ii = 0, J2ii = 0, JXii = 0;
-    int qcrystal = 0;
+    int qcrystal = 0, pbc_off = 0, qct_rm_pbc = 0;
 
     int geom_id() const
     {
@@ -120,7 +120,8 @@ struct Settings {
             if (geom == g[i]) return i;
         return -1;
     }
-    bool c3() const { return geom != "square" && geom != "lieb"; }   // C3SYM, subrouts.cpp:1093-1096
+    // C3SYM, subrouts.cpp:1093-1096 (never for a quasi-crystal)
+    bool c3() const { return !qcrystal && geom != "square" && geom != "lieb"; }
     bool disorder() const { return imp_ratio > 0.0; }
     bool j2_on() const
     {
@@ -158,6 +159,8 @@ struct Settings {
             const int v = std::stoi(c[2 * i + 1]);
             if (v != 0 && v != 1) throw Fail("invalid code-exec setting " + c[2 * i]);
             if (std::string(kCodeSettings[i]) == "qcrystal") qcrystal = v;
+            if (std::string(kCodeSettings[i]) == "PBC_OFF") pbc_off = v;
+            if (std::string(kCodeSettings[i]) == "qct_RemovePBC") qct_rm_pbc = v;
         }
         auto m = tokens(dir + "/Settings_MODEL.txt", 11);
         L = std::stoi(m[0]);
@@ -195,10 +198,18 @@ struct Settings {
     // the input checks of convert_inputs2data and main that apply to SMD
     void validate(bool check_dwf) const
     {
-        if (geom_id() < 0) throw Fail("unknown geometry " + geom);
-        if (qcrystal) throw Fail("quasicrystal inputs are not supported");
-        if (L % 2) throw Fail("lattice length must be a multiple of 2");
-        if (c3() && L % 3) throw Fail("lattice length must be a multiple of 3");
+        if (qcrystal) {
+            // latSize is the site count of an approximant (subrouts.cpp:
+            // 1005-1114); the run needs PBC_OFF = 1 and qct_RemovePBC = 0
+            // (smd_code.cpp:365-372)
+            if (geom != "Aamman") throw Fail("unknown quasi-geometry " + geom);
+            if (qct_rm_pbc || !pbc_off) throw Fail("qcrystal needs PBC_OFF = 1 and qct_RemovePBC = 0");
+            if (L < 4) throw Fail("quasi-crystal size too small");
+        } else {
+            if (geom_id() < 0) throw Fail("unknown geometry " + geom);
+            if (L % 2) throw Fail("lattice length must be a multiple of 2");
+            if (c3() && L % 3) throw Fail("lattice length must be a multiple of 3");
+        }
         if (not_zero(J2_delta) && geom != "lieb") throw Fail("J2_delta requires the lieb geometry");
         if (NMeas % kBinSz || NMeas / kBinSz == 1) throw Fail("NMeas must be a multiple of BinSz with more than one bin");
         if (crSkip <= 0 || kBinSz % crSkip || crSkip > kBinSz) throw Fail("crSkip must divide BinSz");
@@ -616,6 +627,51 @@ void write_text(const Settings &s, const std::string &dir, const std::string &ta
     }
 }
 
+// The autocorrelation file alone (smd_code.cpp:4019-4033): the text spectra
+// of the output stage assume a Bravais grid and are written for crystals only.
+void write_corr(const std::string &dir, const std::string &tag, int ntm, double dtm_rec,
+                const std::vector<double> &qss)
+{
+    const std::string mcr = dir + "/outData/MC_Results/";
+    mkdirs(mcr);
+    std::ofstream f(mcr + "SpinSpin_Temporal_Corr" + tag + ".dat");
+    for (int n = 0; n < ntm; n++) f << sci(n * dtm_rec, 8, 15) << "    " << sci(qss[n], 12, 22) << "\n";
+}
+
+// A quasi-crystal's tables from outBin/ (smd_code.cpp:1248-1300 and
+// 1575-1660): sitesList (N x 2 doubles) and nborsList (per site Zn1, Zn2,
+// ZnX int32, -1 ghosts), exact sizes, unit nearest-neighbour spacing
+// (check_latticeSpc, subrouts.cpp:5803-5832: entries > 0 of site 0).
+void read_qct_tables(const std::string &dir, int N, const int zn[3], std::vector<double> &rvec,
+                     std::vector<int> nb[3])
+{
+    const std::string tag = "_AppxtSz(" + std::to_string(N) + ")";
+    const std::string sites = dir + "/outBin/sitesList" + tag + ".bin", nbors = dir + "/outBin/nborsList" + tag + ".bin";
+    std::ifstream fs(sites, std::ios::binary | std::ios::ate), fn(nbors, std::ios::binary | std::ios::ate);
+    const int zt = zn[0] + zn[1] + zn[2];
+    if (!fs || (size_t)fs.tellg() != (size_t)N * 16) throw Fail("invalid or missing " + sites);
+    if (!fn || (size_t)fn.tellg() != (size_t)N * zt * 4) throw Fail("invalid or missing " + nbors);
+    fs.seekg(0);
+    fn.seekg(0);
+    fs.read(reinterpret_cast<char *>(rvec.data()), (std::streamsize)N * 16);
+    std::vector<int> row((size_t)zt);
+    for (int i = 0; i < N; i++) {
+        fn.read(reinterpret_cast<char *>(row.data()), (std::streamsize)zt * 4);
+        int o = 0;
+        for (int k = 0; k < 3; k++)
+            for (int q = 0; q < zn[k]; q++, o++) {
+                if (row[o] >= N) throw Fail(nbors + ": neighbour index out of range");
+                nb[k][(size_t)i * zn[k] + q] = row[o];
+            }
+    }
+    double lspc = 100.0;
+    for (int q = 0; q < zn[0]; q++) {
+        const int j = nb[0][q];
+        if (j > 0) lspc = std::min(lspc, std::hypot(rvec[2 * j] - rvec[0], rvec[2 * j + 1] - rvec[1]));
+    }
+    if (lspc < 0.95 || lspc > 1.05) throw Fail("lattice spacing is not unit");
+}
+
 int usage()
 {
     std::cerr << "usage: xsmd WORKDIR [--device D] [--precision fp64|fp32] [--stride S] [--fix-every F]"
@@ -672,7 +728,19 @@ int main(int argc, char **argv)
         if (stride < 1 || fix_every < 1) throw Fail("stride and correction period must be positive");
         const std::string tag = s.tag();
         int N = 0, G = 0, nsubs = 0, zn[3] = {0, 0, 0};
-        check(smd_geometry_info(s.geom_id(), s.L, &N, &G, &nsubs, zn), nullptr, "smd_geometry_info");
+        if (s.qcrystal) {
+            // Ammann-Beenker tables: Zn = (8, 3, 8) (subrouts.cpp:1006-1012);
+            // the direct-sum q set is Lsz x Lsz, Lsz the even integer below
+            // sqrt(N) (subrouts.cpp:1111)
+            N = s.L;
+            zn[0] = 8;
+            zn[1] = 3;
+            zn[2] = 8;
+            nsubs = 1;
+            G = ((int)std::sqrt((double)N) / 2) * 2;
+        } else {
+            check(smd_geometry_info(s.geom_id(), s.L, &N, &G, &nsubs, zn), nullptr, "smd_geometry_info");
+        }
         const int n_rec = stride == 1 ? s.ntm : (s.ntm - 1) / stride + 1;
         const int Q = G * G;
         std::vector<double> spec((size_t)3 * Q * n_rec), qss((size_t)n_rec);
@@ -699,9 +767,11 @@ int main(int argc, char **argv)
             std::vector<double> rvec((size_t)N * 2);
             std::vector<int> gmap((size_t)Q), nb[3];
             for (int k = 0; k < 3; k++) nb[k].assign((size_t)N * zn[k], -1);
-            check(smd_build_lattice(s.geom_id(), s.L, rvec.data(), gmap.data(), nb[0].data(), nb[1].data(),
-                                    nb[2].data()),
-                  nullptr, "smd_build_lattice");
+            if (s.qcrystal) read_qct_tables(dir, N, zn, rvec, nb);
+            else
+                check(smd_build_lattice(s.geom_id(), s.L, rvec.data(), gmap.data(), nb[0].data(), nb[1].data(),
+                                        nb[2].data()),
+                      nullptr, "smd_build_lattice");
             const int maxb = N * (zn[0] + zn[1] + zn[2]);
             std::vector<int> bonds((size_t)maxb * 2);
             int nbonds[4];
@@ -739,14 +809,31 @@ int main(int argc, char **argv)
             d.h = s.h;
             for (int k = 0; k < 3; k++) d.nbonds[k] = nbonds[k + 1];
             d.bonds = bonds.data();
-            d.G = G;
-            d.grid_map = gmap.data();
+            d.G = s.qcrystal ? 0 : G;
+            d.grid_map = s.qcrystal ? nullptr : gmap.data();
             d.pos = rvec.data();
             int lid = 0, qid = 0;
             check(smd_lattice_upload(ctx, &d, &lid), ctx, "smd_lattice_upload");
-            check(smd_qset_upload(ctx, lid, 1, 0, nullptr, 1.0, &qid), ctx, "smd_qset_upload");
-            // the static pre-pass over every sample (smd_code.cpp:2289-2726)
-            {
+            if (s.qcrystal) {
+                // get_qct_SqData (subrouts.cpp:8460-8525): index j Lsz + i
+                // holds q = dq (nx(i), ny(j)), n in FFT order, dq = 4 pi2 / Lsz
+                // (smd_code.cpp:1774), scale 1 / sqrt(N)
+                std::vector<double> ql((size_t)Q * 2);
+                const double dq = 4.0 * kPi2 / G;
+                for (int jy = 0; jy < G; jy++)
+                    for (int ix = 0; ix < G; ix++) {
+                        const int nx = ix < G / 2 ? ix : ix - G, ny = jy < G / 2 ? jy : jy - G;
+                        ql[((size_t)jy * G + ix) * 2] = nx * dq;
+                        ql[((size_t)jy * G + ix) * 2 + 1] = ny * dq;
+                    }
+                check(smd_qset_upload(ctx, lid, 0, Q, ql.data(), 1.0 / std::sqrt((double)N), &qid), ctx,
+                      "smd_qset_upload");
+            } else {
+                check(smd_qset_upload(ctx, lid, 1, 0, nullptr, 1.0, &qid), ctx, "smd_qset_upload");
+            }
+            // the static pre-pass over every sample (smd_code.cpp:2289-2726);
+            // a quasi-crystal's runs over the direct-sum q set, not built here
+            if (!s.qcrystal) {
                 std::vector<double> sf((size_t)3 * Q);
                 std::vector<long long> hist(201 * 3);
                 double r0 = 0.0;
@@ -782,7 +869,8 @@ int main(int argc, char **argv)
             f.write(reinterpret_cast<const char *>(qss.data()), (std::streamsize)n_rec * 8);
         }
         const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-        write_text(s, dir, tag, G, n_rec, s.dtm * stride, spec, qss);
+        if (s.qcrystal) write_corr(dir, tag, n_rec, s.dtm * stride, qss);
+        else write_text(s, dir, tag, G, n_rec, s.dtm * stride, spec, qss);
         std::cout << "{\"samples\": " << n << ", \"N\": " << N << ", \"Q\": " << Q << ", \"records\": " << n_rec
                   << ", \"precision\": \"" << (prec == SMD_FP32 ? "fp32" : "fp64") << "\", \"stride\": " << stride
                   << ", \"fix_every\": " << fix_every << ", \"resumed\": " << (s.RecVd1 == 2 ? "true" : "false")

@@ -156,3 +156,47 @@ def test_full_run_reproduces_reference_outputs(tmp_path, xsmd_bin, name):
             ra = [x for x in ref.decode().split() if x != "NaN"]
             assert got.decode().count("NaN") == ref.decode().count("NaN"), k
             assert np.allclose(np.array(ga, float), np.array(ra, float), rtol=2e-5, atol=1e-14), k
+
+
+@pytest.mark.gpu
+def test_quasicrystal_run_reproduces_the_reference_spectrum(tmp_path, xsmd_bin):
+    """qcrystal = 1: the 239-site approximant's tables in outBin/ (the
+    reference's binary layouts), the direct-sum q set of get_qct_SqData:
+    MC_Bin_SpecData within 1e-10 of the reference's sample average (the read
+    window rescaled by its maximum, as the reference does) and the
+    autocorrelation file written."""
+    s, d = load_golden("spec_qct239_open")
+    import dataclasses
+    n = int(d["n"])
+    s = dataclasses.replace(s, window="wread", NMeas=1000 * max(2, n), crSkip=1000)
+    wd = str(tmp_path)
+    s.write(wd)
+    ob = os.path.join(wd, "outBin")
+    os.makedirs(ob, exist_ok=True)
+    smp.write_sample_file(os.path.join(ob, smp.sample_file_name(s)), s, np.asarray(d["spins0"][:n]), None)
+    np.asarray(d["window"], np.float64).tofile(os.path.join(ob, "winvec.bin"))
+    tag = s.size_tag
+    np.asarray(d["rvec"], np.float64).tofile(os.path.join(ob, f"sitesList{tag}.bin"))
+    np.concatenate([d["nb1"], d["nb2"], d["nbx"]], axis=1).astype(np.int32).tofile(
+        os.path.join(ob, f"nborsList{tag}.bin"))
+    r = subprocess.run([xsmd_bin, wd, "--no-dwf-guard"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    Q, ntm = s.G * s.G, s.ntm
+    raw = np.fromfile(os.path.join(ob, "MC_Bin_SpecData" + s.t_tag + ".bin"))
+    spec = raw[: 3 * Q * ntm].reshape(Q, 3, ntm).transpose(1, 0, 2)
+    wmax = float(np.max(d["window"]))
+    ref = d["spec_sum"] / n / (wmax * wmax)
+    assert np.max(np.abs(spec - ref)) <= 1e-10 * np.max(np.abs(ref))
+    assert np.max(np.abs(raw[3 * Q * ntm:] - d["qss_sum"] / n)) <= 1e-10
+    corr = os.path.join(wd, "outData", "MC_Results", "SpinSpin_Temporal_Corr" + s.t_tag + ".dat")
+    assert len(open(corr).read().splitlines()) == ntm
+
+
+def test_quasicrystal_settings_are_checked_as_the_reference_does(tmp_path, xsmd_bin):
+    """A quasi-crystal directory with PBC_OFF = 0 is refused (smd_code.cpp:
+    365-372), before any device work."""
+    s = SMDSettings(geom="Aamman", L=239, NMeas=2000, ntm=16)
+    s.flags["qcrystal"] = 1
+    s.write(str(tmp_path))
+    r = subprocess.run([xsmd_bin, str(tmp_path), "--no-dwf-guard"], capture_output=True, text=True)
+    assert r.returncode == 1 and "PBC_OFF" in r.stderr
