@@ -31,7 +31,7 @@ __device__ __forceinline__ void dft4(cplx<T> &a, cplx<T> &b, cplx<T> &c, cplx<T>
 }
 
 // In-register forward DFT of radix R (sign -1).  For R outside
-// {2, 3, 4, 8, 16} the twiddle table of the full length n
+// {2, 3, 4, 5, 8, 16} the twiddle table of the full length n
 // (tw[j] = exp(-2 pi i j / n)) gives the R-th roots.
 template <typename T, int R>
 __device__ __forceinline__ void dft_small(cplx<T> (&v)[R], const cplx<T> *tw, int n)
@@ -57,6 +57,27 @@ __device__ __forceinline__ void dft_small(cplx<T> (&v)[R], const cplx<T> *tw, in
         v[0] = cadd(a, s);
         v[1] = {m.x + h * d.y, m.y - h * d.x};
         v[2] = {m.x - h * d.y, m.y + h * d.x};
+    } else if constexpr (R == 5) {
+        // w = exp(-2 pi i / 5): with t1 = x1 + x4, t2 = x2 + x3,
+        // t3 = x1 - x4, t4 = x2 - x3 and c_k = cos(2 pi k / 5),
+        // s_k = sin(2 pi k / 5):
+        //   X1, X4 = x0 + c1 t1 + c2 t2 -/+ i (s1 t3 + s2 t4)
+        //   X2, X3 = x0 + c2 t1 + c1 t2 -/+ i (s2 t3 - s1 t4)
+        const T c1 = T(0.30901699437494742410), c2 = T(-0.80901699437494742410);
+        const T s1 = T(0.95105651629515357212), s2 = T(0.58778525229247312917);
+        const cplx<T> x0 = v[0];
+        const cplx<T> t1 = cadd(v[1], v[4]), t2 = cadd(v[2], v[3]);
+        const cplx<T> t3 = csub(v[1], v[4]), t4 = csub(v[2], v[3]);
+        const cplx<T> a1 = {x0.x + c1 * t1.x + c2 * t2.x, x0.y + c1 * t1.y + c2 * t2.y};
+        const cplx<T> a2 = {x0.x + c2 * t1.x + c1 * t2.x, x0.y + c2 * t1.y + c1 * t2.y};
+        const cplx<T> b1 = {s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y};
+        const cplx<T> b2 = {s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y};
+        v[0] = {x0.x + t1.x + t2.x, x0.y + t1.y + t2.y};
+        // -i b = (b.y, -b.x)
+        v[1] = {a1.x + b1.y, a1.y - b1.x};
+        v[4] = {a1.x - b1.y, a1.y + b1.x};
+        v[2] = {a2.x + b2.y, a2.y - b2.x};
+        v[3] = {a2.x - b2.y, a2.y + b2.x};
     } else if constexpr (R == 8) {
         // 8 = 2 x 4: radix-4 over r1 (r = r0 + 2 r1), twiddle w8^(r0 p0),
         // radix-2 over r0; X[p0 + 4 p1] lands in v[2 p0 + p1]
@@ -206,10 +227,32 @@ __device__ __noinline__ void stockham_stage_generic(cplx<T> *buf, int n, int nse
 
 // Stage sets a transform kernel is built with (FL flags), so that each plan
 // pays only for the stages it uses: radix 4 and 2 always run inline;
-// FK_R16 adds inline radix 16 and 8, FK_R3 inline radix 3, and FK_GEN runs
+// FK_R16 adds inline radix 16 and 8, FK_R3 inline radix 3, FK_R5 inline
+// radix 5 (only in plans that need no out-of-line stage; in the others radix
+// 5 runs out of line too, and the instances without radix 5 keep their
+// register budgets), and FK_GEN runs
 // any other radix through the out-of-line streaming stage (whose register
 // needs stay apart from the rest; it needs a scratch copy of the sequences).
-enum { FK_R3 = 1, FK_GEN = 2, FK_R16 = 4 };
+enum { FK_R3 = 1, FK_GEN = 2, FK_R16 = 4, FK_R5 = 8, FK_OOL = 16 };
+
+// FK_OOL: the inline stages are called out of line.  A runtime plan's kernel
+// holds every stage variant behind one switch; inlined, their registers add
+// up and spill, out of line each variant is allocated on its own (one call
+// per stage and batch).
+template <typename T, int R, int NB>
+__device__ __noinline__ void stockham_stage_ool(cplx<T> *buf, int n, int nseq, int ss, int es,
+                                                int Ns, const cplx<T> *tw)
+{
+    stockham_stage<T, R, NB>(buf, n, nseq, ss, es, Ns, tw);
+}
+
+template <typename T, int R, int NB, int FL>
+__device__ __forceinline__ void run_stage(cplx<T> *buf, int n, int nseq, int ss, int es, int Ns,
+                                          const cplx<T> *tw)
+{
+    if constexpr ((FL & FK_OOL) != 0) stockham_stage_ool<T, R, NB>(buf, n, nseq, ss, es, Ns, tw);
+    else stockham_stage<T, R, NB>(buf, n, nseq, ss, es, Ns, tw);
+}
 
 // Full transform.  C = values each thread holds in registers during a
 // stage.  Radices come from the host plan (product = n); every stage needs
@@ -222,18 +265,24 @@ __device__ void smem_fft(cplx<T> *buf, int n, int nseq, int ss, int es, const in
     for (int s = 0; s < nst; s++) {
         const int R = radix[s];
         switch (R) {
-        case 4: stockham_stage<T, 4, (C + 3) / 4>(buf, n, nseq, ss, es, Ns, tw); break;
-        case 2: stockham_stage<T, 2, (C + 1) / 2>(buf, n, nseq, ss, es, Ns, tw); break;
+        case 4: run_stage<T, 4, (C + 3) / 4, FL>(buf, n, nseq, ss, es, Ns, tw); break;
+        case 2: run_stage<T, 2, (C + 1) / 2, FL>(buf, n, nseq, ss, es, Ns, tw); break;
         case 16:
-            if constexpr ((FL & FK_R16) != 0) stockham_stage<T, 16, (C + 15) / 16>(buf, n, nseq, ss, es, Ns, tw);
+            if constexpr ((FL & FK_R16) != 0) run_stage<T, 16, (C + 15) / 16, FL>(buf, n, nseq, ss, es, Ns, tw);
             break;
         case 8:
-            if constexpr ((FL & FK_R16) != 0) stockham_stage<T, 8, (C + 7) / 8>(buf, n, nseq, ss, es, Ns, tw);
+            if constexpr ((FL & FK_R16) != 0) run_stage<T, 8, (C + 7) / 8, FL>(buf, n, nseq, ss, es, Ns, tw);
             break;
         default:
             if constexpr ((FL & FK_R3) != 0) {
                 if (R == 3) {
-                    stockham_stage<T, 3, (C + 2) / 3>(buf, n, nseq, ss, es, Ns, tw);
+                    run_stage<T, 3, (C + 2) / 3, FL>(buf, n, nseq, ss, es, Ns, tw);
+                    break;
+                }
+            }
+            if constexpr ((FL & FK_R5) != 0) {
+                if (R == 5) {
+                    run_stage<T, 5, (C + 4) / 5, FL>(buf, n, nseq, ss, es, Ns, tw);
                     break;
                 }
             }
@@ -263,8 +312,11 @@ inline int fft_plan_flags(const FFTPlan &p)
         const int r = p.radix[s];
         if (r == 16 || r == 8) fl |= FK_R16;
         else if (r == 3) fl |= FK_R3;
+        else if (r == 5) fl |= FK_R5;
         else if (r != 2 && r != 4) fl |= FK_GEN;
     }
+    // radix 5 runs inline only in plans without an out-of-line radix
+    if ((fl & FK_GEN) && (fl & FK_R5)) fl &= ~FK_R5;
     return fl;
 }
 

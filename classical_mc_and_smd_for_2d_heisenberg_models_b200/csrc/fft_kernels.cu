@@ -431,6 +431,7 @@ __global__ void sum_rows_kernel(const double *__restrict__ rows, int W, int n,
 template <typename T>
 static auto time_kernel(int fl)
 {
+    if (fl & FK_R5) return time_fft_kernel<T, FK_R3 | FK_R5>;
     switch (fl & (FK_R3 | FK_GEN)) {
     case 0: return time_fft_kernel<T, 0>;
     case FK_R3: return time_fft_kernel<T, FK_R3>;

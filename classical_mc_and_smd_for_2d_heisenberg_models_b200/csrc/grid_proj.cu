@@ -17,7 +17,11 @@
 // between components are transformed too and never read), both free of bank
 // conflicts.  Each thread holds 16 values per stage.  Common
 // grid sizes run a compile-time radix sequence (48 = 16 x 3, 128 = 16 x 8,
-// ...), the others the runtime plan.
+// ...), the others the runtime plan, whose kernel calls its stages out of
+// line, holds 8 values per thread and transforms the rows (then the
+// columns) in batches of at most 8 x blockDim.x values: the sequences
+// of a pass are independent, so a grid larger than the threads' registers
+// (one component of a 144 x 144 grid, 20736 values) still takes one block.
 #include "fft_device.cuh"
 
 #include <algorithm>
@@ -35,7 +39,7 @@ __device__ __forceinline__ void smem_fft_fixed(cplx<T> *buf, int n, int nseq, in
 
 // blockIdx.x = pair * (3 / NG) + component group, blockIdx.y = sample.
 // P1 > 0: the plan is (P1, P2) at compile time; else the runtime plan with
-// the stage set FL.
+// the stage set FL, in batches of sequences.
 template <typename TS, typename T, int FL, int P1, int P2, int MAXT, int MINB>
 __global__ void __launch_bounds__(MAXT, MINB) grid_proj_kernel(
     const TS *__restrict__ snap, int N, int R, int nrec_chunk, int rec_begin, int n_rec_total,
@@ -57,7 +61,7 @@ __global__ void __launch_bounds__(MAXT, MINB) grid_proj_kernel(
     const TS *x1 = x0 + 3 * (size_t)N;   // the next slot
     for (int k = threadIdx.x; k < G; k += blockDim.x) tw[k] = tw_g[k];
     // one grid-map load serves the NG components of both records
-#pragma unroll 2
+#pragma unroll 4
     for (int rem = threadIdx.x; rem < GG; rem += blockDim.x) {
         const int idx = grid_map[rem];
         const int r = rem / G, col = rem - r * G;
@@ -80,8 +84,13 @@ __global__ void __launch_bounds__(MAXT, MINB) grid_proj_kernel(
         smem_fft_fixed<T, 16, P1, P2>(buf, G, NG * G, P, 1, tw);        // rows
         smem_fft_fixed<T, 16, P1, P2>(buf, G, NG * P - 1, 1, NG * P, tw);   // columns
     } else {
-        smem_fft<T, 16, FL>(buf, G, NG * G, P, 1, plan.radix, plan.nst, tw, scratch, scr_seqs);
-        smem_fft<T, 16, FL>(buf, G, NG * P - 1, 1, NG * P, plan.radix, plan.nst, tw, scratch, scr_seqs);
+        const int cap = max(1, 8 * (int)blockDim.x / G);    // sequences per batch
+        for (int q0 = 0; q0 < NG * G; q0 += cap)            // rows
+            smem_fft<T, 8, FL>(buf + (size_t)q0 * P, G, min(cap, NG * G - q0), P, 1, plan.radix,
+                               plan.nst, tw, scratch, scr_seqs);
+        for (int q0 = 0; q0 < NG * P - 1; q0 += cap)        // columns
+            smem_fft<T, 8, FL>(buf + q0, G, min(cap, NG * P - 1 - q0), 1, NG * P, plan.radix,
+                               plan.nst, tw, scratch, scr_seqs);
     }
     const int t0 = rec_begin + slot0;
     const T sc0 = T(scale * win[t0]), sc1 = has1 ? T(scale * win[t0 + 1]) : T(0);
@@ -150,6 +159,7 @@ __global__ void __launch_bounds__(512) grid_rows_kernel(
     const TS *x0 = snap + ((size_t)(s * R + slot0) * 3 + c) * N;
     const TS *x1 = x0 + 3 * (size_t)N;
     for (int k = threadIdx.x; k < G; k += blockDim.x) tw[k] = tw_g[k];
+#pragma unroll 4
     for (int e = threadIdx.x; e < RT * G; e += blockDim.x) {
         const int rr = e / G, col = e - rr * G;
         T a = T(0), b = T(0);
@@ -193,6 +203,7 @@ __global__ void __launch_bounds__(512) grid_cols_kernel(
     const cplx<T> *z = Zg + (((size_t)s * ((R + 1) / 2) + pair) * 3 + c) * G * G;
     for (int k = threadIdx.x; k < G; k += blockDim.x) tw[k] = tw_g[k];
     // columns j < CT: kc = c0 + j; columns CT + j: their mirrors
+#pragma unroll 4
     for (int e = threadIdx.x; e < G * W2; e += blockDim.x) {
         const int x = e / W2, j = e - x * W2;
         const int jj = j < CT ? j : j - CT;
@@ -252,15 +263,32 @@ constexpr auto fixed_kernel()
     return grid_proj_kernel<T, T, FK_R16 | (P2 == 3 ? FK_R3 : 0), P1, P2, MAXT, MINB>;
 }
 
+// Runtime plans: stages out of line, sequences in batches, 64 registers a
+// thread; launched with up to 512 threads while two blocks fit an SM's
+// shared memory (the blocks' phases overlap), else up to 1024 (measured on
+// honeycomb, kagome, square and triangular grids of 36 to 144 points).
+constexpr int kRuntimeThreads = 1024;
+constexpr size_t kTwoBlockSmem = 113 * 1024;
+
 template <typename T>
 auto runtime_kernel(int fl)
 {
+    constexpr int M = kRuntimeThreads, O = FK_OOL | FK_R16;
+    if (fl & FK_R5) return grid_proj_kernel<T, T, O | FK_R3 | FK_R5, 0, 1, M, 1>;
     switch (fl & (FK_R3 | FK_GEN)) {
-    case 0: return grid_proj_kernel<T, T, FK_R16, 0, 1, 1024, 1>;
-    case FK_R3: return grid_proj_kernel<T, T, FK_R16 | FK_R3, 0, 1, 1024, 1>;
-    case FK_GEN: return grid_proj_kernel<T, T, FK_R16 | FK_GEN, 0, 1, 1024, 1>;
-    default: return grid_proj_kernel<T, T, FK_R16 | FK_R3 | FK_GEN, 0, 1, 1024, 1>;
+    case 0: return grid_proj_kernel<T, T, O, 0, 1, M, 1>;
+    case FK_R3: return grid_proj_kernel<T, T, O | FK_R3, 0, 1, M, 1>;
+    case FK_GEN: return grid_proj_kernel<T, T, O | FK_GEN, 0, 1, M, 1>;
+    default: return grid_proj_kernel<T, T, O | FK_R3 | FK_GEN, 0, 1, M, 1>;
     }
+}
+
+// whether a plan runs a compile-time radix sequence
+static bool fixed_plan(const FFTPlan &p)
+{
+    const int r1 = p.nst > 0 ? p.radix[0] : 0, r2 = p.nst > 1 ? p.radix[1] : 1;
+    if (p.nst > 2) return false;
+    return (r1 == 16 && (r2 == 1 || r2 == 2 || r2 == 3 || r2 == 4 || r2 == 8)) || (r1 == 8 && r2 == 3);
 }
 
 // the kernel for a plan: a compile-time radix sequence when one matches
@@ -296,7 +324,9 @@ static int grid_scratch_seqs(int G, int ng, const FFTPlan &p)
 
 // Components per block: all three while their values fit 512 threads of
 // 16 values and the shared memory of two blocks per SM (FP32) or one (FP64),
-// else one.  0: the grid does not fit one block.
+// else one while the component's grid fits the shared memory of a block (a
+// compile-time plan also needs its values to fit 1024 threads of 16; the
+// runtime kernel batches its sequences).  0: the grid does not fit one block.
 static size_t grid_smem_ng(int G, int ng, int precision, const FFTPlan &p)
 {
     const size_t e = precision == 0 ? sizeof(cplx<double>) : sizeof(cplx<float>);
@@ -307,7 +337,8 @@ int grid_proj_ng(int G, int precision, const FFTPlan &p)
 {
     const size_t cap3 = (precision == 0 ? 200 : 110) * 1024;
     if (grid_work(G, 3) <= 16 * 512 && grid_smem_ng(G, 3, precision, p) <= cap3) return 3;
-    if (grid_work(G, 1) <= 16 * 1024 && grid_smem_ng(G, 1, precision, p) <= 200 * 1024) return 1;
+    if (fixed_plan(p) && grid_work(G, 1) > 16 * 1024) return 0;
+    if (grid_smem_ng(G, 1, precision, p) <= 220 * 1024) return 1;
     return 0;
 }
 
@@ -359,11 +390,14 @@ cudaError_t launch_grid_proj_large(const void *snap, int precision, int N, int W
     const size_t sm_c = large_smem(G, G * (2 * CT + 1), precision, plan, &scr_c);
     const int thr_r = fft_threads(RT * (G + 1), 8), thr_c = fft_threads(G * (2 * CT + 1), 8);
     const dim3 gr(pairs * 3 * ((G + RT - 1) / RT), W), gc(pairs * 3 * ((G + CT - 1) / CT), W);
-    const bool gen = plan_generic(plan);
+    const bool gen = plan_generic(plan), r5 = (fft_plan_flags(plan) & FK_R5) != 0;
     if (precision == 0) {
         auto kr = gen ? grid_rows_kernel<double, double, FK_R16 | FK_R3 | FK_GEN>
+                : r5  ? grid_rows_kernel<double, double, FK_R16 | FK_R3 | FK_R5>
                       : grid_rows_kernel<double, double, FK_R16 | FK_R3>;
-        auto kc = gen ? grid_cols_kernel<double, FK_R16 | FK_R3 | FK_GEN> : grid_cols_kernel<double, FK_R16 | FK_R3>;
+        auto kc = gen ? grid_cols_kernel<double, FK_R16 | FK_R3 | FK_GEN>
+                : r5  ? grid_cols_kernel<double, FK_R16 | FK_R3 | FK_R5>
+                      : grid_cols_kernel<double, FK_R16 | FK_R3>;
         allow_dynamic_smem(kr);
         allow_dynamic_smem(kc);
         kr<<<gr, thr_r, sm_r, st>>>((const double *)snap, N, R, nrec_chunk, grid_map, plan,
@@ -373,8 +407,11 @@ cudaError_t launch_grid_proj_large(const void *snap, int precision, int N, int W
                                     scr_c);
     } else {
         auto kr = gen ? grid_rows_kernel<float, float, FK_R16 | FK_R3 | FK_GEN>
+                : r5  ? grid_rows_kernel<float, float, FK_R16 | FK_R3 | FK_R5>
                       : grid_rows_kernel<float, float, FK_R16 | FK_R3>;
-        auto kc = gen ? grid_cols_kernel<float, FK_R16 | FK_R3 | FK_GEN> : grid_cols_kernel<float, FK_R16 | FK_R3>;
+        auto kc = gen ? grid_cols_kernel<float, FK_R16 | FK_R3 | FK_GEN>
+                : r5  ? grid_cols_kernel<float, FK_R16 | FK_R3 | FK_R5>
+                      : grid_cols_kernel<float, FK_R16 | FK_R3>;
         allow_dynamic_smem(kr);
         allow_dynamic_smem(kc);
         kr<<<gr, thr_r, sm_r, st>>>((const float *)snap, N, R, nrec_chunk, grid_map, plan,
@@ -395,7 +432,9 @@ cudaError_t launch_grid_proj(const void *snap, int precision, int N, int W, int 
     const int ng = grid_proj_ng(G, precision, plan);
     if (!ng) return cudaErrorInvalidValue;
     const size_t smem = grid_proj_smem(G, precision, plan);
-    const int threads = fft_threads((int)grid_work(G, ng), 16);
+    const int threads = fixed_plan(plan) ? fft_threads((int)grid_work(G, ng), 16)
+                                         : std::min(fft_threads((int)grid_work(G, ng), 8),
+                                                    smem <= kTwoBlockSmem ? 512 : kRuntimeThreads);
     dim3 grid(((nrec_chunk + 1) / 2) * (3 / ng), W);
     if (precision == 0) {
         GridKernelD k = pick_kernel<double>(plan);

@@ -162,9 +162,10 @@ def test_two_pass_grid_transform_vs_oracle(ctx, oracle_mod, monkeypatch, geom, L
 
 @pytest.mark.parametrize("precision", [_lib.SMD_FP64, _lib.SMD_FP32])
 def test_grid_larger_than_one_block(ctx, oracle_mod, precision):
-    """Honeycomb L = 48 (N = 4608, a 144 x 144 grid, beyond one block): the
-    two-pass transform against the oracle (FP64 within 1e-10, FP32 form
-    within 1e-3 rel-L2)."""
+    """Honeycomb L = 48 (N = 4608, a 144 x 144 grid): the FP64 form takes the
+    two-pass transform (beyond one block's shared memory), the FP32 form one
+    block per component with its rows and columns in three batches each;
+    against the oracle (FP64 within 1e-10, FP32 form within 1e-3 rel-L2)."""
     s = SMDSettings(geom="hexagn", L=48, J2=0.2, dtm=0.01, ntm=16, window="hann1")
     lat, lid = _upload(ctx, s)
     qid = ctx.qset(lid, use_grid=True)
@@ -176,6 +177,34 @@ def test_grid_larger_than_one_block(ctx, oracle_mod, precision):
     acc = 0.0
     for k in range(2):
         acc = acc + oracle_mod.dyn_spectrum(m, spins[k], s.dtm, 16, win=win)["spec"]
+    acc /= 2
+    if precision == _lib.SMD_FP64:
+        assert np.max(np.abs(r.spec - acc)) <= SPEC_TOL * np.max(np.abs(acc))
+    else:
+        assert np.linalg.norm(r.spec - acc) / np.linalg.norm(acc) <= 1e-3
+
+
+@pytest.mark.parametrize("two_pass", [False, True])
+@pytest.mark.parametrize("precision", [_lib.SMD_FP64, _lib.SMD_FP32])
+def test_radix5_grid_and_time_transforms_vs_oracle(ctx, oracle_mod, monkeypatch, precision, two_pass):
+    """Honeycomb L = 30: a 90 x 90 grid (radices 2, 3, 3, 5) in one block and
+    through the two-pass transform, and 50 records (radices 2, 5, 5): the
+    inline radix-5 stages against the oracle (FP64 within 1e-10, FP32 form
+    within 1e-3 rel-L2)."""
+    if two_pass:
+        monkeypatch.setenv("SMD_GRID_TWO_PASS", "1")
+    s = SMDSettings(geom="hexagn", L=30, J2=0.2, JX=0.05, dtm=0.01, ntm=50, window="hann1")
+    lat, lid = _upload(ctx, s)
+    assert lat.G == 90
+    qid = ctx.qset(lid, use_grid=True)
+    spins, _ = smp.make_samples(s, 2, "ferro", 0.4, 17)
+    win = smd.window("hann1", 50)
+    kw = dict(precision=precision, fix_every=16) if precision == _lib.SMD_FP32 else {}
+    r = ctx.run(lid, qid, spins, s.dtm, 50, win=win, **kw)
+    m = oracle_mod.Model(s, oracle_mod.make_lattice("hexagn", 30))
+    acc = 0.0
+    for k in range(2):
+        acc = acc + oracle_mod.dyn_spectrum(m, spins[k], s.dtm, 50, win=win)["spec"]
     acc /= 2
     if precision == _lib.SMD_FP64:
         assert np.max(np.abs(r.spec - acc)) <= SPEC_TOL * np.max(np.abs(acc))
