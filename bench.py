@@ -420,10 +420,13 @@ def run_ours(args, w, rank, world):
             raise _lib.SMDError(rc, lib.smd_last_error(ctx.h).decode())
         return t1 - t0
 
-    e2e_steps = max(1, min(args.steps, 3))
+    # K steps, each from the host buffers to the host result; the mean step
+    # time (one step's wall time moves by tens of ms with the host's load:
+    # the 277 MB spectrum crosses PCIe every step)
+    e2e_steps = max(1, args.steps)
     e2e_step()
     e2e_t = [e2e_step() for _ in range(e2e_steps)]
-    tt = torch.tensor([max(e2e_t)], dtype=torch.float64, device=f"cuda:{local}")
+    tt = torch.tensor([sum(e2e_t) / len(e2e_t)], dtype=torch.float64, device=f"cuda:{local}")
     if dist is not None:
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
     e2e_value = site_steps_rank * world / float(tt.item())
@@ -640,7 +643,8 @@ def run_batch(args, bw, rank, world):
         return t1 - t0
 
     e2e()
-    e2e_t = max(e2e() for _ in range(max(1, min(args.steps, 3))))
+    e2e_k = max(1, args.steps)
+    e2e_t = sum(e2e() for _ in range(e2e_k)) / e2e_k   # mean step time over K steps
     e2e_value = site_steps_rank * world / e2e_t
 
     # FP64 plain form: every member alone through smd_run_device, FP64,
@@ -884,6 +888,9 @@ def main():
                     help="override the record count (small profiling cases only)")
     ap.add_argument("--samples", type=int, default=0,
                     help="override the samples per GPU (small profiling cases only)")
+    ap.add_argument("--lattice", default="",
+                    help="GEOM:L, override the lattice (profiling a lattice shape only; "
+                         "ordered state ferro except triangular 120-degree and square stripe)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -940,6 +947,10 @@ def main():
             w = dataclasses.replace(w, n_rec=args.records)
         if args.samples:
             w = dataclasses.replace(w, n_samples=args.samples)
+        if args.lattice:
+            geom, L = args.lattice.split(":")
+            w = dataclasses.replace(w, settings=dataclasses.replace(w.settings, geom=geom, L=int(L)),
+                                    state={"triang": "q120", "square": "stripe"}.get(geom, "ferro"))
     if args.impl == "reference":
         line = run_reference_arm(args, w, rank, world)
     else:

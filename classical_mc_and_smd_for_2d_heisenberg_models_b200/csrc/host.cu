@@ -684,11 +684,45 @@ int project_chunk(smd_ctx *ctx, const ProjArgs &a, cudaStream_t st, int *launche
     return SMD_OK;
 }
 
+// Estimated RK time of a cluster shape, in units of one site's stage work at
+// full SM throughput: the busiest SM runs ceil(CTAs / SMs) CTAs, k at a time
+// (k from registers, shared memory and threads); a round of j CTAs of
+// w warps each runs at min(1, j w / 20) of the SM's throughput; a CTA's work
+// is its own sites plus half a site per halo copy, times 1.2 for four sites a
+// thread (128 registers, spills), plus 60 site-units per CTA of the cluster
+// (cluster-wide waits).  The constants were fitted to the RK times of every
+// shape of twelve serving-mix jobs (five geometries, N 432-6084, 46-253
+// samples): the shapes it picks ran within 3 % of the fastest measured per
+// job, against 13 % for the fill rule below (9 % leaving each job out of
+// the fit in turn).
+static double shape_cost(const ClusterParams &P, int prec, int spt, int threads, int n_samples, int sms)
+{
+    const int regs = spt == 1 ? 80 : spt == 2 ? 96 : 128;   // the instances' register counts
+    const int warps = threads / 32;
+    const size_t smem = rk_cluster_smem(P, prec) + 1024;
+    int k = std::min({65536 / (threads * regs), (int)((228 * 1024) / smem), 2048 / threads});
+    k = std::max(k, 1);
+    const long long ctas = (long long)n_samples * P.CS;
+    long long rem = (ctas + sms - 1) / sms;
+    double rounds = 0.0;
+    while (rem > 0) {
+        const int j = (int)std::min<long long>(k, rem);
+        rounds += j / std::min(1.0, j * warps / 20.0);
+        rem -= j;
+    }
+    const double spt_factor = spt == 4 ? 1.2 : 1.0;
+    const double work = (P.n_own_max + 0.5 * (P.n_loc_max - P.n_own_max)) * spt_factor + 60.0 * P.CS;
+    return rounds * work;
+}
+
 // Cluster size and thread shape for a job.  Lattices the cluster kernel does
 // not cover (bond-list energies, the Lieb d-wave term, impurities with
-// non-zero couplings) keep the single-CTA kernel.  Otherwise the smallest
-// cluster that puts at least ~85% of the SMs to work is taken, within the
-// shared-memory and register limits; SMD_CLUSTER_CTAS forces a size.
+// non-zero couplings) keep the single-CTA kernel.  Otherwise the shape of
+// least estimated time (shape_cost) over every cluster size and
+// sites-per-thread form that fits the shared-memory and register limits.
+// SMD_CLUSTER_POLICY=fill takes instead the smallest cluster that puts at
+// least ~85% of the SMs to work; SMD_CLUSTER_CTAS forces a size (with
+// SMD_RK_SPT forcing the sites per thread).
 ClusterTab *cluster_choice(Lattice &L, int prec, int n_samples, int device, int *spt_out, int *threads_out)
 {
     if (!cluster_ok(L)) return nullptr;
@@ -696,6 +730,38 @@ ClusterTab *cluster_choice(Lattice &L, int prec, int n_samples, int device, int 
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     int forced = 0;
     if (const char *e = std::getenv("SMD_CLUSTER_CTAS")) forced = std::atoi(e);
+    const char *pol = std::getenv("SMD_CLUSTER_POLICY");
+    if (!forced && !(pol && std::strcmp(pol, "fill") == 0)) {
+        ClusterTab *best = nullptr;
+        double best_cost = 0.0;
+        for (int CS : {1, 2, 4, 8, 16}) {
+            if (CS > 1 && L.N / CS < 96) break;
+            ClusterTab *t = cluster_tables(L, CS);
+            if (!t || rk_cluster_smem(t->P, prec) > 227 * 1024) continue;
+            for (int s : {1, 2, 4}) {
+                if (s * rk_cluster_maxt(prec, s) < t->P.n_own_max) continue;
+                const int thr = std::min(std::max(32, (t->P.n_own_max + s - 1) / s + 31) / 32 * 32,
+                                         rk_cluster_maxt(prec, s));
+                const double c = shape_cost(t->P, prec, s, thr, n_samples, sms);
+                if (const char *tr = std::getenv("SMD_CLUSTER_TRACE")) {
+                    // candidate shapes and their estimates, appended to a file
+                    if (FILE *f = std::fopen(tr, "a")) {
+                        std::fprintf(f, "N %d S %d CS %d spt %d thr %d own %d loc %d smem %zu cost %.1f\n", L.N,
+                                     n_samples, CS, s, thr, t->P.n_own_max, t->P.n_loc_max,
+                                     rk_cluster_smem(t->P, prec), c);
+                        std::fclose(f);
+                    }
+                }
+                if (!best || c < best_cost * 0.98) {
+                    best = t;
+                    best_cost = c;
+                    *spt_out = s;
+                    *threads_out = thr;
+                }
+            }
+        }
+        return best;
+    }
     ClusterTab *best = nullptr;
     const int sizes[] = {1, 2, 4, 8, 16};
     for (int CS : sizes) {
@@ -821,6 +887,8 @@ int prepare(smd_ctx *ctx, const smd_job_desc *job, JobGeom &g)
     W = std::min<size_t>(W, 65535);
     g.W = (int)W;
     g.waves = (job->n_samples + g.W - 1) / g.W;
+    // the RK launches run one wave of W samples at a time: shape them for W
+    if (g.ctab && g.W < job->n_samples) choose_cluster(ctx, g, g.W);
     return SMD_OK;
 }
 

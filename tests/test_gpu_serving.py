@@ -66,13 +66,15 @@ def test_jobs_of_different_lengths_overlap():
         jobs = _jobs(ctx)
         s, lid, qid, sp, _ = jobs[4]
         long_w = smd.window("hann1", 4096)
-        long_id = ctx.submit(lid, qid, sp, s.dtm, 4096, stride=16, win=long_w, **kw)
+        # 262 080 steps: long enough that the short jobs' first kernel loads
+        # and admissions cannot outlast it
+        long_id = ctx.submit(lid, qid, sp, s.dtm, 4096, stride=64, win=long_w, **kw)
         short = [ctx.submit(l2, q2, sp2, s2.dtm, 32, stride=2, win=w2, **kw)
                  for s2, l2, q2, sp2, w2 in jobs[:4]]
         short_res = [ctx.wait(j) for j in short]
         assert ctx.poll(long_id) == _lib.SMD_EBUSY
         long_res = ctx.wait(long_id)
-        alone = ctx.wait(ctx.submit(lid, qid, sp, s.dtm, 4096, stride=16, win=long_w, **kw))
+        alone = ctx.wait(ctx.submit(lid, qid, sp, s.dtm, 4096, stride=64, win=long_w, **kw))
         assert np.array_equal(long_res[0], alone[0])
         for (s2, l2, q2, sp2, w2), r in zip(jobs[:4], short_res):
             a2 = ctx.wait(ctx.submit(l2, q2, sp2, s2.dtm, 32, stride=2, win=w2, **kw))
