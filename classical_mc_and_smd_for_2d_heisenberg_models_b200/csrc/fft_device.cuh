@@ -237,66 +237,52 @@ enum { FK_R3 = 1, FK_GEN = 2, FK_R16 = 4, FK_R5 = 8, FK_OOL = 16 };
 
 // FK_OOL: the inline stages are called out of line.  A runtime plan's kernel
 // holds every stage variant behind one switch; inlined, their registers add
-// up and spill, out of line each variant is allocated on its own.  One call
-// runs a stage over every batch of sequences, so a pass costs one call (and
-// its register saves) per stage.
-
-// One stage over nseq sequences in batches of at most cap (the sequences
-// are independent; batch b starts at sequence b * cap).
+// up and spill, out of line each variant is allocated on its own (one call
+// per stage and batch).
 template <typename T, int R, int NB>
-__device__ __forceinline__ void stockham_batches(cplx<T> *buf, int n, int nseq, int cap, int ss, int es,
-                                                 int Ns, const cplx<T> *tw)
+__device__ __noinline__ void stockham_stage_ool(cplx<T> *buf, int n, int nseq, int ss, int es,
+                                                int Ns, const cplx<T> *tw)
 {
-    for (int q0 = 0; q0 < nseq; q0 += cap)
-        stockham_stage<T, R, NB>(buf + (size_t)q0 * ss, n, min(cap, nseq - q0), ss, es, Ns, tw);
-}
-
-template <typename T, int R, int NB>
-__device__ __noinline__ void stockham_batches_ool(cplx<T> *buf, int n, int nseq, int cap, int ss, int es,
-                                                  int Ns, const cplx<T> *tw)
-{
-    stockham_batches<T, R, NB>(buf, n, nseq, cap, ss, es, Ns, tw);
+    stockham_stage<T, R, NB>(buf, n, nseq, ss, es, Ns, tw);
 }
 
 template <typename T, int R, int NB, int FL>
-__device__ __forceinline__ void run_stage(cplx<T> *buf, int n, int nseq, int cap, int ss, int es, int Ns,
+__device__ __forceinline__ void run_stage(cplx<T> *buf, int n, int nseq, int ss, int es, int Ns,
                                           const cplx<T> *tw)
 {
-    if constexpr ((FL & FK_OOL) != 0) stockham_batches_ool<T, R, NB>(buf, n, nseq, cap, ss, es, Ns, tw);
-    else stockham_batches<T, R, NB>(buf, n, nseq, cap, ss, es, Ns, tw);
+    if constexpr ((FL & FK_OOL) != 0) stockham_stage_ool<T, R, NB>(buf, n, nseq, ss, es, Ns, tw);
+    else stockham_stage<T, R, NB>(buf, n, nseq, ss, es, Ns, tw);
 }
 
 // Full transform.  C = values each thread holds in registers during a
-// stage.  Radices come from the host plan (product = n); the inline stages
-// take the sequences in batches of cap (default: all at once), and every
-// batch needs cap * n <= C * blockDim.x.
+// stage.  Radices come from the host plan (product = n); every stage needs
+// nseq * n <= C * blockDim.x.
 template <typename T, int C, int FL>
 __device__ void smem_fft(cplx<T> *buf, int n, int nseq, int ss, int es, const int *radix,
-                         int nst, const cplx<T> *tw, cplx<T> *scratch, int scr_seqs, int cap = 0)
+                         int nst, const cplx<T> *tw, cplx<T> *scratch, int scr_seqs)
 {
-    if (cap <= 0) cap = nseq;
     int Ns = 1;
     for (int s = 0; s < nst; s++) {
         const int R = radix[s];
         switch (R) {
-        case 4: run_stage<T, 4, (C + 3) / 4, FL>(buf, n, nseq, cap, ss, es, Ns, tw); break;
-        case 2: run_stage<T, 2, (C + 1) / 2, FL>(buf, n, nseq, cap, ss, es, Ns, tw); break;
+        case 4: run_stage<T, 4, (C + 3) / 4, FL>(buf, n, nseq, ss, es, Ns, tw); break;
+        case 2: run_stage<T, 2, (C + 1) / 2, FL>(buf, n, nseq, ss, es, Ns, tw); break;
         case 16:
-            if constexpr ((FL & FK_R16) != 0) run_stage<T, 16, (C + 15) / 16, FL>(buf, n, nseq, cap, ss, es, Ns, tw);
+            if constexpr ((FL & FK_R16) != 0) run_stage<T, 16, (C + 15) / 16, FL>(buf, n, nseq, ss, es, Ns, tw);
             break;
         case 8:
-            if constexpr ((FL & FK_R16) != 0) run_stage<T, 8, (C + 7) / 8, FL>(buf, n, nseq, cap, ss, es, Ns, tw);
+            if constexpr ((FL & FK_R16) != 0) run_stage<T, 8, (C + 7) / 8, FL>(buf, n, nseq, ss, es, Ns, tw);
             break;
         default:
             if constexpr ((FL & FK_R3) != 0) {
                 if (R == 3) {
-                    run_stage<T, 3, (C + 2) / 3, FL>(buf, n, nseq, cap, ss, es, Ns, tw);
+                    run_stage<T, 3, (C + 2) / 3, FL>(buf, n, nseq, ss, es, Ns, tw);
                     break;
                 }
             }
             if constexpr ((FL & FK_R5) != 0) {
                 if (R == 5) {
-                    run_stage<T, 5, (C + 4) / 5, FL>(buf, n, nseq, cap, ss, es, Ns, tw);
+                    run_stage<T, 5, (C + 4) / 5, FL>(buf, n, nseq, ss, es, Ns, tw);
                     break;
                 }
             }

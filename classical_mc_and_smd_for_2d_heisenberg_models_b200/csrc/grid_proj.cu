@@ -85,9 +85,12 @@ __global__ void __launch_bounds__(MAXT, MINB) grid_proj_kernel(
         smem_fft_fixed<T, 16, P1, P2>(buf, G, NG * P - 1, 1, NG * P, tw);   // columns
     } else {
         const int cap = max(1, 8 * (int)blockDim.x / G);    // sequences per batch
-        smem_fft<T, 8, FL>(buf, G, NG * G, P, 1, plan.radix, plan.nst, tw, scratch, scr_seqs, cap);   // rows
-        smem_fft<T, 8, FL>(buf, G, NG * P - 1, 1, NG * P, plan.radix, plan.nst, tw, scratch, scr_seqs,
-                           cap);                                                                     // columns
+        for (int q0 = 0; q0 < NG * G; q0 += cap)            // rows
+            smem_fft<T, 8, FL>(buf + (size_t)q0 * P, G, min(cap, NG * G - q0), P, 1, plan.radix,
+                               plan.nst, tw, scratch, scr_seqs);
+        for (int q0 = 0; q0 < NG * P - 1; q0 += cap)        // columns
+            smem_fft<T, 8, FL>(buf + q0, G, min(cap, NG * P - 1 - q0), 1, NG * P, plan.radix,
+                               plan.nst, tw, scratch, scr_seqs);
     }
     const int t0 = rec_begin + slot0;
     const T sc0 = T(scale * win[t0]), sc1 = has1 ? T(scale * win[t0 + 1]) : T(0);
