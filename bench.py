@@ -155,7 +155,7 @@ def serving_leg(device: int, n_jobs: int, seed: int, fp64: bool = True):
     geometries, N log-uniform in [256, 16384], 16-256 samples, 2^12-2^15 RK
     steps, 1024 records, FP32 form) through the continuous-batching engine
     (smd_submit / smd_wait).  One burst (every job queued at once) gives the
-    aggregate service rate (median of three bursts); Poisson arrivals at 70 % of it give p50 / p99
+    aggregate service rate (median of five bursts); Poisson arrivals at 70 % of it give p50 / p99
     latency (submit to completion, as the library measures it).  The same
     jobs run one at a time through smd_run in the FP64 plain form give the
     FP64 spectra each served result's DSSF rel-L2 is taken against and one
@@ -208,11 +208,11 @@ def serving_leg(device: int, n_jobs: int, seed: int, fp64: bool = True):
         # time plans and pinned staging are set up on first use
         for j in [submit(p) for p in prepared]:
             ctx.wait(j)
-        # bursts: every job queued at once; the median makespan of three
-        # gives the service rate (one burst's makespan moves by +-10 % from
-        # run to run)
+        # bursts: every job queued at once; the median makespan of five
+        # gives the service rate (one burst's makespan moves by up to 30 %
+        # from burst to burst, the first after the warm-up most)
         spans = []
-        for _ in range(3):
+        for _ in range(5):
             t0 = time.perf_counter()
             ids = [submit(p) for p in prepared]
             burst = [ctx.wait(j) for j in ids]

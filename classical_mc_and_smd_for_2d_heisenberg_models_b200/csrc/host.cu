@@ -497,7 +497,13 @@ ClusterTab *cluster_tables(Lattice &L, int CS, int zt_min)
     if (CS < 1 || CS > kMaxClusterCTAs || N < CS) return nullptr;
     const int zact = L.zn[0] + L.zn[1] + L.zn[2];
     const int zneed = std::max(zact, zt_min);
-    const int ZT = zneed <= 4 ? 4 : zneed <= 8 ? 8 : zneed <= 12 ? 12 : zneed <= 18 ? 18 : zneed <= 20 ? 20 : -1;
+    const int ZT = zneed <= 4    ? 4
+                   : zneed <= 8  ? 8
+                   : zneed <= 12 ? 12
+                   : zneed <= 14 ? 14
+                   : zneed <= 18 ? 18
+                   : zneed <= 20 ? 20
+                                 : -1;
     if (ZT < 0) return nullptr;
     std::lock_guard<std::mutex> lk(L.cache_mu);
     auto it = L.ctabs.find({CS, ZT});

@@ -888,6 +888,7 @@ cudaError_t launch_cluster_spt(const ClusterParams &P, const RKJob &J, int threa
     case 4: return launch_cluster_t<T, SPT, 4>(P, J, threads, smem, st);
     case 8: return launch_cluster_t<T, SPT, 8>(P, J, threads, smem, st);
     case 12: return launch_cluster_t<T, SPT, 12>(P, J, threads, smem, st);
+    case 14: return launch_cluster_t<T, SPT, 14>(P, J, threads, smem, st);
     case 18: return launch_cluster_t<T, SPT, 18>(P, J, threads, smem, st);
     case 20: return launch_cluster_t<T, SPT, 20>(P, J, threads, smem, st);
     default: return cudaErrorInvalidValue;
