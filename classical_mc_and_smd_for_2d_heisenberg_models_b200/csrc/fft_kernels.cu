@@ -224,8 +224,15 @@ __host__ __device__ inline int p2_table_size(int log2n)
 // waited for (with the fixed limit kDrainPolls) before the block exits.
 constexpr unsigned kDrainPolls = 1u << 26;   // about a second of polling
 
-template <typename T>
-__global__ void __launch_bounds__(sizeof(T) == 8 ? 256 : 512) time_fft_pow2_kernel(
+// INPLACE (the FP32 form): one tile buffer that the passes also work in
+// (the copy lands in natural order, the first pass reads it all before
+// writing the swizzled layout back), 64 registers a thread, so two blocks
+// share an SM and one block's copy overlaps the other's passes; the copy of
+// sample s + 1 is issued once the last pass of sample s has read the buffer.
+// Otherwise a tile buffer and a work buffer, one block per SM, and the copy
+// of sample s + 1 issued after the first pass of sample s.
+template <typename T, bool INPLACE>
+__global__ void __launch_bounds__(sizeof(T) == 8 ? 256 : 512, INPLACE ? 2 : 1) time_fft_pow2_kernel(
     const cplx<T> *__restrict__ series, int W, int Q, int nqb, int n, int log2n, int nseq,
     const cplx<T> *__restrict__ tw_g, double *__restrict__ acc, int *status, unsigned poll_limit)
 {
@@ -238,7 +245,7 @@ __global__ void __launch_bounds__(sizeof(T) == 8 ? 256 : 512) time_fft_pow2_kern
     const int PS = n + (QB == 2 ? 8 : 0);
     const int n16 = log2n >> 2, rl = 1 << (log2n & 3);
     cplx<T> *S = reinterpret_cast<cplx<T> *>(smem_raw);
-    cplx<T> *Wb = S + (size_t)nseq * n;
+    cplx<T> *Wb = INPLACE ? S : S + (size_t)nseq * n;
     cplx<T> *ts = Wb + (size_t)nseq * PS;
     uint64_t *bar = reinterpret_cast<uint64_t *>(ts + p2_table_size(log2n));
     __shared__ int abort_flag;
@@ -322,7 +329,7 @@ __global__ void __launch_bounds__(sizeof(T) == 8 ? 256 : 512) time_fft_pow2_kern
             for (int r = 0; r < 16; r++) v[r] = src[(size_t)r * m * QB];
         }
         __syncthreads();   // S consumed; Wb free (the previous sample's last pass has read it)
-        if (threadIdx.x == 0 && s + 1 < W) issue(s + 1);
+        if ((!INPLACE || nst == 1) && threadIdx.x == 0 && s + 1 < W) issue(s + 1);
         dft_small<T, 16>(v, ts, n);   // no table lookups at radix 16
         if (nst == 1) {
             p2_accumulate<T, 16>(v, a, inv_n);
@@ -362,6 +369,10 @@ __global__ void __launch_bounds__(sizeof(T) == 8 ? 256 : 512) time_fft_pow2_kern
         if (rl == 2) p2_last<T, 2>(v, a, Wb, tp, n, PS, Ns, inv_n);
         else if (rl == 4) p2_last<T, 4>(v, a, Wb, tp, n, PS, Ns, inv_n);
         else if (rl == 8) p2_last<T, 8>(v, a, Wb, tp, n, PS, Ns, inv_n);
+        if constexpr (INPLACE) {
+            __syncthreads();   // the last pass has read the buffer
+            if (threadIdx.x == 0 && s + 1 < W) issue(s + 1);
+        }
     }
     if (abort_flag) {
         // the copy in flight (sample s_abort) lands before the block exits
@@ -463,12 +474,15 @@ static int pow2_nseq(int n, int precision, int Q)
     return nseq < qb ? qb : nseq / qb * qb;
 }
 
+// the FP32 form's kernel works in its tile buffer (INPLACE), the FP64 one
+// has a tile buffer and a work buffer
 static size_t pow2_smem(int n, int nseq, int precision)
 {
     const size_t e = precision == 0 ? sizeof(cplx<double>) : sizeof(cplx<float>);
     const int qb = series_qblock(precision);
     const size_t ps = (size_t)n + (qb == 2 ? 8 : 0);
-    return ((size_t)nseq * n + (size_t)nseq * ps + p2_table_size(pow2_log2(n))) * e + 16;
+    const size_t tile = precision == 0 ? (size_t)nseq * n : 0;
+    return (tile + (size_t)nseq * ps + p2_table_size(pow2_log2(n))) * e + 16;
 }
 
 // sequences per block of the generic transform: a multiple of the q block,
@@ -515,12 +529,12 @@ cudaError_t launch_time_fft(const void *series, int precision, int W, int Q, int
         const int threads = nseq * n / 16;
         const int ntile = (nqb * qb + nseq - 1) / nseq;
         if (precision == 0) {
-            auto k = time_fft_pow2_kernel<double>;
+            auto k = time_fft_pow2_kernel<double, false>;
             allow_dynamic_smem(k);
             k<<<ncomp * ntile, threads, smem, st>>>((const cplx<double> *)series, W, Q, nqb, n, l2, nseq,
                                                 (const cplx<double> *)tw, acc, status, polls);
         } else {
-            auto k = time_fft_pow2_kernel<float>;
+            auto k = time_fft_pow2_kernel<float, true>;
             allow_dynamic_smem(k);
             k<<<ncomp * ntile, threads, smem, st>>>((const cplx<float> *)series, W, Q, nqb, n, l2, nseq,
                                                 (const cplx<float> *)tw, acc, status, polls);
